@@ -1,0 +1,291 @@
+// Batched dense block operations on the diagonal / all blocks of a block-sparse matrix.
+#include <algorithm>
+
+#include "blockops.cuh"
+
+namespace bsgpu {
+
+namespace {
+
+__device__ __forceinline__ int64_t diag_block(const int64_t* rp, const int32_t* ci, int64_t i) {
+  for (int64_t k = rp[i]; k < rp[i + 1]; ++k)
+    if (ci[k] == i) return k;
+  return -1;
+}
+
+__device__ __forceinline__ double packed_at(const double* v, int64_t boff, int I, int V, int r, int c) {
+  return v[boff + (int64_t)(c / V) * I * V + r * V + (c % V)];
+}
+
+// One CTA per block row: symmetric elimination of the diagonal block in shared memory.
+// Row/column scalings and additions are those of SymmInv; the additions of one elimination step are applied
+// together as M <- E M E^T, L <- E L with E = I + sum_k a_k e_k e_i^T (the elementary operations of one step
+// commute, so this equals the reference's sequential order up to rounding).
+__global__ void symminv_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                               const int32_t* __restrict__ len, const int64_t* __restrict__ boff,
+                               const double* __restrict__ vals, int V, const int64_t* __restrict__ doff,
+                               double* __restrict__ Lout, int* __restrict__ err, int64_t nb) {
+  extern __shared__ double sm[];
+  for (int64_t i = blockIdx.x; i < nb; i += gridDim.x) {
+    const int n = len[i];
+    double* M = sm;
+    double* L = sm + n * n;
+    double* rowi = L + n * n;
+    double* coli = rowi + n;
+    double* a = coli + n;
+    __shared__ int bad;
+    const int64_t kd = diag_block(rp, ci, i);
+    if (threadIdx.x == 0) bad = (kd < 0);
+    __syncthreads();
+    if (bad) {
+      if (threadIdx.x == 0) atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff));
+      __syncthreads();
+      continue;
+    }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e - r * n;
+      M[e] = packed_at(vals, boff[kd], n, V, r, c);
+      L[e] = (r == c) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int p = 0; p < n; ++p) {
+      const double Mpp = M[p * n + p];
+      if (Mpp == 0.0 || !isfinite(Mpp)) {
+        if (threadIdx.x == 0) { bad = 1; atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff)); }
+        __syncthreads();
+        break;
+      }
+      const double scl = 1.0 / sqrt(fabs(Mpp));
+      for (int c = threadIdx.x; c < n; c += blockDim.x) {
+        M[p * n + c] *= scl;
+        L[p * n + c] *= scl;
+      }
+      __syncthreads();
+      for (int r = threadIdx.x; r < n; r += blockDim.x) M[r * n + p] *= scl;
+      __syncthreads();
+      const double d = M[p * n + p];
+      const double sgn = d > 0 ? 1.0 : -1.0;
+      if (fabs(fabs(d) - 1.0) > 1.0e-8) {
+        if (threadIdx.x == 0) { bad = 1; atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff)); }
+        __syncthreads();
+        break;
+      }
+      for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        rowi[q] = M[p * n + q];
+        coli[q] = M[q * n + p];
+        a[q] = (q > p) ? -M[q * n + p] * sgn : 0.0;
+      }
+      __syncthreads();
+      const double mpp = M[p * n + p];
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        M[e] += a[r] * rowi[c] + a[c] * coli[r] + a[r] * a[c] * mpp;
+        if (r > p) L[e] += a[r] * L[p * n + c];
+      }
+      __syncthreads();
+    }
+    double* out = Lout + doff[i];
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) out[e] = L[e];
+    __syncthreads();
+  }
+}
+
+// Aout(k) = L_i A(k) L_j^T, one CTA per block, L lower triangular.
+__global__ void cob_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                           const int32_t* __restrict__ len, const int32_t* __restrict__ blk_row,
+                           const int64_t* __restrict__ boff_in, int Vin, const double* __restrict__ vin,
+                           const int64_t* __restrict__ boff_out, int Vout, double* __restrict__ vout,
+                           const double* __restrict__ L, const int64_t* __restrict__ doff, int64_t nnzb) {
+  extern __shared__ double sm[];
+  for (int64_t k = blockIdx.x; k < nnzb; k += gridDim.x) {
+    const int i = blk_row[k], j = ci[k];
+    const int I = len[i], J = len[j];
+    double* A = sm;
+    double* T = A + I * J;
+    double* Li = T + I * J;
+    double* Lj = Li + I * I;
+    for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+      const int r = e / J, c = e - r * J;
+      A[e] = packed_at(vin, boff_in[k], I, Vin, r, c);
+    }
+    for (int e = threadIdx.x; e < I * I; e += blockDim.x) Li[e] = L[doff[i] + e];
+    for (int e = threadIdx.x; e < J * J; e += blockDim.x) Lj[e] = L[doff[j] + e];
+    __syncthreads();
+    for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+      const int r = e / J, c = e - r * J;
+      double s = 0.0;
+      for (int q = 0; q <= r; ++q) s = fma(Li[r * I + q], A[q * J + c], s);
+      T[e] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+      const int r = e / J, c = e - r * J;
+      double s = 0.0;
+      for (int q = 0; q <= c; ++q) s = fma(T[r * J + q], Lj[c * J + q], s);
+      vout[boff_out[k] + (int64_t)(c / Vout) * I * Vout + r * Vout + (c % Vout)] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// Gauss-Jordan inversion with partial pivoting of the diagonal block, one CTA per block row.
+__global__ void invert_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                              const int32_t* __restrict__ len, const int64_t* __restrict__ boff,
+                              const double* __restrict__ vals, int V, const int64_t* __restrict__ doff,
+                              double* __restrict__ D64, float* __restrict__ D32, int* __restrict__ err, int64_t nb) {
+  extern __shared__ double sm[];
+  for (int64_t i = blockIdx.x; i < nb; i += gridDim.x) {
+    const int n = len[i];
+    double* M = sm;
+    double* prow = sm + n * n;
+    double* pcol = prow + n;
+    int* perm = reinterpret_cast<int*>(pcol + n);
+    __shared__ int piv;
+    __shared__ int bad;
+    const int64_t kd = diag_block(rp, ci, i);
+    if (threadIdx.x == 0) bad = (kd < 0);
+    __syncthreads();
+    if (bad) {
+      if (threadIdx.x == 0) atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff));
+      __syncthreads();
+      continue;
+    }
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e - r * n;
+      M[e] = packed_at(vals, boff[kd], n, V, r, c);
+    }
+    __syncthreads();
+    for (int p = 0; p < n; ++p) {
+      if (threadIdx.x == 0) {
+        int best = p;
+        double mx = fabs(M[p * n + p]);
+        for (int r = p + 1; r < n; ++r)
+          if (fabs(M[r * n + p]) > mx) { mx = fabs(M[r * n + p]); best = r; }
+        piv = best;
+        perm[p] = best;
+        if (!(mx > 0.0) || !isfinite(mx)) { bad = 1; atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff)); }
+      }
+      __syncthreads();
+      if (bad) break;
+      if (piv != p)
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+          const double t = M[p * n + c];
+          M[p * n + c] = M[piv * n + c];
+          M[piv * n + c] = t;
+        }
+      __syncthreads();
+      const double inv = 1.0 / M[p * n + p];
+      for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        prow[q] = (q == p) ? inv : M[p * n + q] * inv;
+        pcol[q] = M[q * n + p];
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        if (r == p)
+          M[e] = prow[c];
+        else if (c == p)
+          M[e] = -pcol[r] * prow[p];
+        else
+          M[e] -= pcol[r] * prow[c];
+      }
+      __syncthreads();
+    }
+    if (!bad) {
+      // undo the row interchanges as column interchanges, in reverse order
+      for (int p = n - 1; p >= 0; --p) {
+        const int q = perm[p];
+        if (q != p)
+          for (int r = threadIdx.x; r < n; r += blockDim.x) {
+            const double t = M[r * n + p];
+            M[r * n + p] = M[r * n + q];
+            M[r * n + q] = t;
+          }
+        __syncthreads();
+      }
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        const double v = M[r * n + c];
+        if (D64) D64[doff[i] + (int64_t)c * n + r] = v;
+        if (D32) D32[doff[i] + (int64_t)c * n + r] = (float)v;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// y_i = L_i^{-T} x_i, one thread per block row (back substitution with the upper-triangular L^T)
+__global__ void trsv_lt_kernel(const int32_t* __restrict__ len, const int64_t* __restrict__ i0,
+                               const int64_t* __restrict__ doff, const double* __restrict__ L,
+                               const double* __restrict__ x, double* __restrict__ y, int64_t nb) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (int64_t)gridDim.x * blockDim.x) {
+    const int n = len[i];
+    const double* Li = L + doff[i];
+    const int64_t s0 = i0[i];
+    for (int r = n - 1; r >= 0; --r) {
+      double s = x[s0 + r];
+      for (int c = r + 1; c < n; ++c) s -= Li[c * n + r] * y[s0 + c];
+      y[s0 + r] = s / Li[r * n + r];
+    }
+  }
+}
+
+DBuf<int32_t> blk_rows(const Matrix& A) {
+  std::vector<int32_t> br(A.nnzb);
+  for (int64_t i = 0; i < A.nb; ++i)
+    for (int64_t k = A.h_rp[i]; k < A.h_rp[i + 1]; ++k) br[k] = (int32_t)i;
+  DBuf<int32_t> d(std::max<int64_t>(A.nnzb, 1));
+  if (A.nnzb) BSGPU_CUDA(cudaMemcpy(d.p, br.data(), A.nnzb * 4, cudaMemcpyHostToDevice));
+  return d;
+}
+
+int grid_for(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(n, (int64_t)num_sms() * 16)); }
+
+}  // namespace
+
+void symminv_batched(const Matrix& A, double* L, int* err, cudaStream_t st) {
+  require(!A.single, "SymmInv needs the FP64 matrix");
+  if (A.nb == 0) return;
+  const int64_t n = A.max_len();
+  const size_t smem = (size_t)(2 * n * n + 3 * n) * sizeof(double);
+  require(smem <= 200 * 1024, "block too large for SymmInv", BSGPU_ERR_UNSUPPORTED);
+  if (smem > 48 * 1024) BSGPU_CUDA(cudaFuncSetAttribute(symminv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  symminv_kernel<<<grid_for(A.nb), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, A.doff.p, L, err,
+                                                   A.nb);
+  BSGPU_CHECK_LAUNCH();
+}
+
+void change_of_basis_apply(const Matrix& A, const double* L, Matrix& Aout, cudaStream_t st) {
+  require(!A.single && !Aout.single, "change of basis needs FP64 matrices");
+  if (A.nnzb == 0) return;
+  const int64_t n = A.max_len();
+  const size_t smem = (size_t)(4 * n * n) * sizeof(double);
+  require(smem <= 200 * 1024, "block too large for the change of basis", BSGPU_ERR_UNSUPPORTED);
+  if (smem > 48 * 1024) BSGPU_CUDA(cudaFuncSetAttribute(cob_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  DBuf<int32_t> br = blk_rows(A);
+  cob_kernel<<<grid_for(A.nnzb), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, br.p, A.boff.p, A.V, A.v64.p, Aout.boff.p,
+                                                 Aout.V, Aout.v64.p, L, A.doff.p, A.nnzb);
+  BSGPU_CHECK_LAUNCH();
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+}
+
+void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cudaStream_t st) {
+  require(!A.single, "inversion needs the FP64 matrix");
+  if (A.nb == 0) return;
+  const int64_t n = A.max_len();
+  const size_t smem = (size_t)(n * n + 2 * n) * sizeof(double) + (size_t)n * sizeof(int);
+  require(smem <= 200 * 1024, "block too large for the inversion", BSGPU_ERR_UNSUPPORTED);
+  if (smem > 48 * 1024) BSGPU_CUDA(cudaFuncSetAttribute(invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  invert_kernel<<<grid_for(A.nb), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, A.doff.p, D64, D32,
+                                                  err, A.nb);
+  BSGPU_CHECK_LAUNCH();
+}
+
+void block_trsv_lt(const Matrix& A, const double* L, const double* x, double* y, cudaStream_t st) {
+  if (A.nb == 0) return;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((A.nb + 127) / 128, (int64_t)num_sms() * 8));
+  trsv_lt_kernel<<<grid, 128, 0, st>>>(A.len.p, A.i0.p, A.doff.p, L, x, y, A.nb);
+  BSGPU_CHECK_LAUNCH();
+}
+
+}  // namespace bsgpu

@@ -1,0 +1,18 @@
+// Batched dense block operations: SymmInv change of basis, diagonal-block inversion, block triangular solves.
+#pragma once
+#include "matrix.cuh"
+
+namespace bsgpu {
+
+// L_i for every block row from SymmInv of the diagonal block (MultigridOperator_ChangeOfBasis.cs:624-760).
+// L: per block row I x I row-major at offsets diag_offsets(A).  Returns 0 or the first failing block + 1.
+void symminv_batched(const Matrix& A, double* L, int* err, cudaStream_t st);
+// Aout_ij = L_i * A_ij * L_j^T for every block (Aout has A's structure, FP64).
+void change_of_basis_apply(const Matrix& A, const double* L, Matrix& Aout, cudaStream_t st);
+// Inverses of the diagonal blocks (BlockJacobi.cs:125-146 InvertInPlace), stored column-major per block at
+// diag_offsets(A); computed in FP64 and written as FP64 (D64) and/or FP32 (D32).
+void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cudaStream_t st);
+// y_i = L_i^{-T} x_i per block (initial-guess transform with a lower-triangular L, row-major).
+void block_trsv_lt(const Matrix& A, const double* L, const double* x, double* y, cudaStream_t st);
+
+}  // namespace bsgpu

@@ -1,0 +1,353 @@
+// extern "C" boundary of the library (declarations and reference citations in include/bsgpu.h).
+#include <atomic>
+#include <cstring>
+#include <memory>
+
+#include "solvers.cuh"
+
+struct bsgpu_matrix_s {
+  std::unique_ptr<bsgpu::Matrix> m;
+  bool borrowed = false;
+  bsgpu::Matrix* get() { return m.get(); }
+};
+
+struct bsgpu_mgop_s {
+  bsgpu::Matrix* A = nullptr;  // original operator (owned by the caller's handle)
+  std::unique_ptr<bsgpu::Matrix> Aop;
+  bsgpu::DBuf<double> L;       // per-block left change of basis, row-major
+  int mode = 0;
+  bsgpu_matrix_s op_handle;    // borrowed handle returned by bsgpu_mgop_get_operator
+  const bsgpu::Matrix* op() const { return mode == BSGPU_COB_EYE ? A : Aop.get(); }
+};
+
+struct bsgpu_solver_s {
+  bsgpu_mgop_s* op = nullptr;
+  std::unique_ptr<bsgpu::Tree> tree;
+  bsgpu::DBuf<double> X, B, Xt, Bt;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  std::vector<double> history;
+};
+
+namespace bsgpu {
+
+thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+static std::atomic<unsigned long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return BSGPU_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host allocation failed");
+    return BSGPU_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return BSGPU_ERR_ARGUMENT;
+  }
+}
+
+// transformed RHS / initial guess and back-transform (MultigridOperator.TransformRhsInto / TransformSolFrom)
+void to_transformed(bsgpu_mgop_s* op, const double* X, const double* B, double* Xt, double* Bt, cudaStream_t st) {
+  const Matrix& A = *op->A;
+  if (op->mode == BSGPU_COB_EYE) {
+    BSGPU_CUDA(cudaMemcpyAsync(Bt, B, A.N * 8, cudaMemcpyDeviceToDevice, st));
+    BSGPU_CUDA(cudaMemcpyAsync(Xt, X, A.N * 8, cudaMemcpyDeviceToDevice, st));
+    return;
+  }
+  block_gemv(op->L.p, A.doff.p, A.len.p, A.i0.p, A.row2blk.p, A.uniform ? A.Np : 0, false, B, Bt, A.N, st);
+  block_trsv_lt(A, op->L.p, X, Xt, st);
+}
+
+void from_transformed(bsgpu_mgop_s* op, const double* Xt, double* X, cudaStream_t st) {
+  const Matrix& A = *op->A;
+  if (op->mode == BSGPU_COB_EYE) {
+    BSGPU_CUDA(cudaMemcpyAsync(X, Xt, A.N * 8, cudaMemcpyDeviceToDevice, st));
+    return;
+  }
+  block_gemv(op->L.p, A.doff.p, A.len.p, A.i0.p, A.row2blk.p, A.uniform ? A.Np : 0, true, Xt, X, A.N, st);
+}
+
+void solve_device(bsgpu_solver_s* s, double* dX, const double* dB, bsgpu_solve_stats* stats) {
+  Tree& t = *s->tree;
+  Ctx& c = *t.ctx;
+  const int64_t N = s->op->A->N;
+  BSGPU_CUDA(cudaEventRecord(s->e0, c.st));
+  to_transformed(s->op, dX, dB, s->Xt.p, s->Bt.p, c.st);
+  t.top->this_level_iterations = 0;
+  t.top->solve(c, s->Xt.p, s->Bt.p, false);
+  from_transformed(s->op, s->Xt.p, dX, c.st);
+  BSGPU_CUDA(cudaEventRecord(s->e1, c.st));
+  BSGPU_CUDA(cudaEventSynchronize(s->e1));
+  float ms = 0;
+  BSGPU_CUDA(cudaEventElapsedTime(&ms, s->e0, s->e1));
+  s->history = t.top->history;
+  if (stats) {
+    stats->iterations = t.top->this_level_iterations;
+    stats->nested = t.top->nested();
+    stats->converged = t.top->converged ? 1 : 0;
+    stats->n_history = (int32_t)s->history.size();
+    stats->res0 = s->history.empty() ? 0.0 : s->history.front();
+    stats->res = s->history.empty() ? 0.0 : s->history.back();
+    stats->seconds = ms * 1e-3;
+  }
+  (void)N;
+}
+
+}  // namespace
+}  // namespace bsgpu
+
+using namespace bsgpu;
+
+extern "C" {
+
+BSGPU_API int bsgpu_get_version(int* major, int* minor) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  return BSGPU_OK;
+}
+
+BSGPU_API int bsgpu_get_launch_count(uint64_t* n) {
+  if (!n) return BSGPU_ERR_ARGUMENT;
+  *n = g_launches.load();
+  return BSGPU_OK;
+}
+
+BSGPU_API int bsgpu_last_error(char* buf, size_t len) {
+  if (!buf || len == 0) return BSGPU_ERR_ARGUMENT;
+  std::strncpy(buf, g_last_error.c_str(), len - 1);
+  buf[len - 1] = '\0';
+  return BSGPU_OK;
+}
+
+BSGPU_API int bsgpu_set_device(int device) {
+  return guarded([&] { BSGPU_CUDA(cudaSetDevice(device)); });
+}
+
+BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, const int32_t* nspc,
+                                  const int64_t* row_ptr, const int32_t* col_idx, const double* values,
+                                  int32_t flags) {
+  return guarded([&] {
+    require(A != nullptr, "null handle pointer");
+    auto h = std::make_unique<bsgpu_matrix_s>();
+    h->m.reset(matrix_create(nb, Np, nspc, row_ptr, col_idx, values, flags));
+    *A = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A) {
+  return guarded([&] {
+    if (A && !A->borrowed) delete A;
+  });
+}
+
+BSGPU_API int bsgpu_matrix_get_info(bsgpu_matrix_t A, int64_t* nrows, int64_t* nb, int64_t* nnzb, int32_t* Np) {
+  return guarded([&] {
+    require(A && A->get(), "null matrix");
+    const Matrix& M = *A->get();
+    if (nrows) *nrows = M.N;
+    if (nb) *nb = M.nb;
+    if (nnzb) *nnzb = M.nnzb;
+    if (Np) *Np = M.Np;
+  });
+}
+
+BSGPU_API int bsgpu_matrix_read_values(bsgpu_matrix_t A, double* values, int32_t flags) {
+  return guarded([&] {
+    require(A && A->get() && values, "null argument");
+    matrix_read_values(*A->get(), values, flags == BSGPU_DEVICE_POINTERS, nullptr);
+  });
+}
+
+BSGPU_API int bsgpu_matrix_spmv(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y) {
+  return guarded([&] {
+    require(A && A->get() && x && y, "null argument");
+    require(x != y, "In-Place computation is not supported.");
+    const Matrix& M = *A->get();
+    DBuf<double> dx(std::max<int64_t>(M.N, 1)), dy(std::max<int64_t>(M.N, 1));
+    if (M.N) {
+      BSGPU_CUDA(cudaMemcpy(dx.p, x, M.N * 8, cudaMemcpyHostToDevice));
+      if (beta != 0.0) BSGPU_CUDA(cudaMemcpy(dy.p, y, M.N * 8, cudaMemcpyHostToDevice));
+    }
+    spmv(M, alpha, dx.p, beta, beta != 0.0 ? dy.p : nullptr, dy.p, nullptr);
+    if (M.N) BSGPU_CUDA(cudaMemcpy(y, dy.p, M.N * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
+BSGPU_API int bsgpu_matrix_spmv_device(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y,
+                                       void* stream) {
+  return guarded([&] {
+    require(A && A->get() && x && y, "null argument");
+    require(x != y, "In-Place computation is not supported.");
+    spmv(*A->get(), alpha, x, beta, beta != 0.0 ? y : nullptr, y, (cudaStream_t)stream);
+  });
+}
+
+BSGPU_API int bsgpu_matrix_create_single(bsgpu_matrix_t A, bsgpu_matrix_t* A32) {
+  return guarded([&] {
+    require(A && A->get() && A32, "null argument");
+    auto h = std::make_unique<bsgpu_matrix_s>();
+    h->m.reset(matrix_to_single(*A->get(), nullptr));
+    *A32 = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_matrix_spmv_device_f32(bsgpu_matrix_t A32, float alpha, const float* x, float beta, float* y,
+                                           void* stream) {
+  return guarded([&] {
+    require(A32 && A32->get() && x && y, "null argument");
+    require(x != y, "In-Place computation is not supported.");
+    spmv(*A32->get(), alpha, x, beta, beta != 0.0f ? y : nullptr, y, (cudaStream_t)stream);
+  });
+}
+
+BSGPU_API int bsgpu_matrix_restrict(bsgpu_matrix_t A, int32_t keep, bsgpu_matrix_t* Asub) {
+  return guarded([&] {
+    require(A && A->get() && Asub, "null argument");
+    auto h = std::make_unique<bsgpu_matrix_s>();
+    h->m.reset(matrix_restrict(*A->get(), keep, nullptr));
+    *Asub = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_mgop_create(bsgpu_mgop_t* op, bsgpu_matrix_t A, int32_t mode) {
+  return guarded([&] {
+    require(op && A && A->get(), "null argument");
+    require(mode == BSGPU_COB_EYE || mode == BSGPU_COB_DIAG_BLOCK_EQUILIB, "unknown change-of-basis mode");
+    require(!A->get()->single, "the operator must be FP64");
+    auto h = std::make_unique<bsgpu_mgop_s>();
+    h->A = A->get();
+    h->mode = mode;
+    if (mode == BSGPU_COB_DIAG_BLOCK_EQUILIB) {
+      const Matrix& M = *h->A;
+      std::vector<int64_t> o = diag_offsets(M);
+      h->L.alloc(std::max<int64_t>(o.back(), 1));
+      DBuf<int> err(1);
+      BSGPU_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+      symminv_batched(M, h->L.p, err.p, nullptr);
+      int herr = 0;
+      BSGPU_CUDA(cudaMemcpy(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+      if (herr)
+        throw Error(BSGPU_ERR_ARITHMETIC, "SymmInv: zero or indefinite pivot in diagonal block " + std::to_string(herr - 1));
+      h->Aop.reset(matrix_like(M, false));
+      change_of_basis_apply(M, h->L.p, *h->Aop, nullptr);
+    }
+    h->op_handle.m.reset(const_cast<Matrix*>(h->op()));
+    h->op_handle.borrowed = true;
+    *op = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_mgop_destroy(bsgpu_mgop_t op) {
+  return guarded([&] {
+    if (!op) return;
+    op->op_handle.m.release();  // borrowed
+    delete op;
+  });
+}
+
+BSGPU_API int bsgpu_mgop_get_operator(bsgpu_mgop_t op, bsgpu_matrix_t* Aop) {
+  return guarded([&] {
+    require(op && Aop, "null argument");
+    *Aop = &op->op_handle;
+  });
+}
+
+BSGPU_API int bsgpu_mgop_read_left_cob(bsgpu_mgop_t op, double* L) {
+  return guarded([&] {
+    require(op && L, "null argument");
+    require(op->mode == BSGPU_COB_DIAG_BLOCK_EQUILIB, "no change of basis (mode Eye)");
+    std::vector<int64_t> o = diag_offsets(*op->A);
+    BSGPU_CUDA(cudaMemcpy(L, op->L.p, o.back() * 8, cudaMemcpyDeviceToHost));
+  });
+}
+
+BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
+  return guarded([&] {
+    require(cfg != nullptr, "null config");
+    std::memset(cfg, 0, sizeof(*cfg));
+    cfg->solver = BSGPU_SOLVER_FGMRES_PMG;
+    cfg->termination = BSGPU_TERM_DEFAULT;
+    cfg->tol = 1e-10;
+    cfg->max_iter = 300;
+    cfg->min_iter = 1;
+    cfg->max_krylov = 30;
+    cfg->n_levels = 1;
+    cfg->post_sweeps = 10;
+    cfg->bj_iters = 1;
+    cfg->bj_omega = 1.0;
+    cfg->coarse_kind = BSGPU_COARSE_PCG;
+    cfg->coarse_tol = 1e-3;
+    cfg->coarse_max_iter = 2000;
+    cfg->sub_max_iter = 100;
+    cfg->sub_reduction = 0.1;
+    cfg->precision = BSGPU_PRECISION_FP64;
+  });
+}
+
+BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgpu_solver_config* cfg) {
+  return guarded([&] {
+    require(s && op && cfg, "null argument");
+    auto h = std::make_unique<bsgpu_solver_s>();
+    h->op = op;
+    h->tree.reset(build_tree(op->op(), *cfg));
+    const int64_t N = std::max<int64_t>(op->A->N, 1);
+    h->X.alloc(N); h->B.alloc(N); h->Xt.alloc(N); h->Bt.alloc(N);
+    BSGPU_CUDA(cudaEventCreate(&h->e0));
+    BSGPU_CUDA(cudaEventCreate(&h->e1));
+    *s = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_solver_destroy(bsgpu_solver_t s) {
+  return guarded([&] {
+    if (!s) return;
+    if (s->e0) cudaEventDestroy(s->e0);
+    if (s->e1) cudaEventDestroy(s->e1);
+    delete s;
+  });
+}
+
+BSGPU_API int bsgpu_solver_solve(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats) {
+  return guarded([&] {
+    require(s && X && B, "null argument");
+    const int64_t N = s->op->A->N;
+    cudaStream_t st = s->tree->ctx->st;
+    if (N) {
+      BSGPU_CUDA(cudaMemcpyAsync(s->B.p, B, N * 8, cudaMemcpyHostToDevice, st));
+      BSGPU_CUDA(cudaMemcpyAsync(s->X.p, X, N * 8, cudaMemcpyHostToDevice, st));
+    }
+    solve_device(s, s->X.p, s->B.p, stats);
+    if (N) {
+      BSGPU_CUDA(cudaMemcpyAsync(X, s->X.p, N * 8, cudaMemcpyDeviceToHost, st));
+      BSGPU_CUDA(cudaStreamSynchronize(st));
+    }
+  });
+}
+
+BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats) {
+  return guarded([&] {
+    require(s && X && B, "null argument");
+    BSGPU_CUDA(cudaDeviceSynchronize());
+    solve_device(s, X, B, stats);
+  });
+}
+
+BSGPU_API int bsgpu_solver_get_history(bsgpu_solver_t s, double* hist, int32_t cap, int32_t* n) {
+  return guarded([&] {
+    require(s != nullptr, "null solver");
+    const int32_t k = (int32_t)s->history.size();
+    if (n) *n = k;
+    if (hist)
+      for (int32_t i = 0; i < k && i < cap; ++i) hist[i] = s->history[i];
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// Device-resident block-sparse matrix (the BlockMsrMatrix of the solver path) and its kernels' launchers.
+//
+// Device layout ("row-interleaved slab").  Block row i, with block length I and occupied blocks k = rp[i] ..
+// rp[i+1]-1 of widths J_k, is one slab of I rows and sum_k J_k columns.  The slab is cut into column chunks of
+// V consecutive entries (V = 2 for FP64 and V = 4 for FP32 when the block widths allow it, else smaller); the
+// chunks are stored chunk-major, row-minor:   value(k, r, c) = boff[k] + (c / V) * I * V + r * V + c % V.
+// A thread that owns DOF row r of block row i therefore streams its row with V-wide vector loads while the
+// I threads of the block row read one contiguous run of I*V values per step: every HBM sector that is fetched
+// is fully used and no shuffle or shared-memory reduction is needed.  Blocks never straddle a chunk because V
+// divides every block width.
+#pragma once
+#include "common.cuh"
+
+namespace bsgpu {
+
+struct Matrix {
+  int64_t nb = 0, N = 0, nnzb = 0;
+  int Np = 0;            // modes per species
+  bool uniform = true;   // every block has Np rows (one species)
+  bool single = false;   // values stored as float
+  int V = 1;             // chunk width (elements)
+  // host copies of the structure
+  std::vector<int64_t> h_rp, h_i0;
+  std::vector<int32_t> h_ci, h_len, h_nspc;
+  // device structure
+  DBuf<int64_t> rp, i0, boff;
+  DBuf<int32_t> ci, len, row2blk;
+  DBuf<int64_t> doff;      // offsets of the per-block-row diagonal factors (I*I each)
+  DBuf<int64_t> cta_row0;  // CTA packing for the variable-size kernels (whole block rows per CTA)
+  int64_t ncta = 0;
+  int cta_threads = 256;
+  DBuf<double> v64;
+  DBuf<float> v32;
+  int64_t nvals = 0;
+
+  size_t value_bytes() const { return (size_t)nvals * (single ? 4 : 8); }
+  int64_t max_len() const;
+};
+
+// Creation from block-CSR arrays with row-major blocks (host or device pointers).
+Matrix* matrix_create(int64_t nb, int32_t Np, const int32_t* nspc, const int64_t* row_ptr, const int32_t* col_idx,
+                      const double* values, int32_t flags);
+// A matrix with the same structure as `A` and values given in the device layout of `A` (used for transforms).
+Matrix* matrix_like(const Matrix& A, bool single);
+void matrix_read_values(const Matrix& A, double* dst, bool dst_device, cudaStream_t st);
+Matrix* matrix_to_single(const Matrix& A, cudaStream_t st);
+Matrix* matrix_restrict(const Matrix& A, int keep, cudaStream_t st);
+
+// y = alpha*A*x + beta*z (z may be y; z == nullptr: beta ignored).  `active`: optional device flag, the launch
+// is a no-op when *active == 0.
+void spmv(const Matrix& A, double alpha, const double* x, double beta, const double* z, double* y, cudaStream_t st,
+          const int* active = nullptr);
+void spmv(const Matrix& A, float alpha, const float* x, float beta, const float* z, float* y, cudaStream_t st,
+          const int* active = nullptr);
+// Block-Jacobi update fused into the SpMV: xo = x + omega * Dinv * (b - A*x).  Dinv: per block row, column-major.
+void bj_update(const Matrix& A, const double* dinv, double omega, const double* x, const double* b, double* xo,
+               cudaStream_t st, const int* active = nullptr);
+void bj_update(const Matrix& A, const float* dinv, float omega, const float* x, const float* b, float* xo,
+               cudaStream_t st, const int* active = nullptr);
+// y = omega * Dinv * b (first block-Jacobi sweep from a zero guess).
+void blockdiag_apply(const Matrix& A, const double* dinv, double omega, const double* b, double* y, cudaStream_t st,
+                     const int* active = nullptr);
+void blockdiag_apply(const Matrix& A, const float* dinv, float omega, const float* b, float* y, cudaStream_t st,
+                     const int* active = nullptr);
+
+// Offsets of the per-block-row dense diagonal factors (column-major I x I each) and their total size.
+std::vector<int64_t> diag_offsets(const Matrix& A);
+
+}  // namespace bsgpu

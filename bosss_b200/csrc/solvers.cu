@@ -1,0 +1,773 @@
+// Solver tree of the hot path (see solvers.cuh).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "solvers.cuh"
+
+namespace bsgpu {
+
+// ---------------------------------------------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------------------------------------------
+Ctx::Ctx() {
+  BSGPU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  dscal.alloc(scal_cap);
+  BSGPU_CUDA(cudaMallocHost(&hscal, scal_cap * sizeof(double)));
+  dflag.alloc(256);
+  BSGPU_CUDA(cudaMemset(dflag.p, 0, 256 * sizeof(int)));
+  BSGPU_CUDA(cudaMemset(dscal.p, 0, scal_cap * sizeof(double)));
+  red.init();
+}
+Ctx::~Ctx() {
+  if (hscal) cudaFreeHost(hscal);
+  if (st) cudaStreamDestroy(st);
+}
+double* Ctx::scal(int n) {
+  require(nscal + n <= scal_cap, "solver tree needs too many device scalars", BSGPU_ERR_UNSUPPORTED);
+  double* p = dscal.p + nscal;
+  nscal += n;
+  return p;
+}
+int* Ctx::flag() {
+  require(nflag < 256, "solver tree needs too many device flags", BSGPU_ERR_UNSUPPORTED);
+  return dflag.p + nflag++;
+}
+void Ctx::fetch(const double* d, int n) {
+  BSGPU_CUDA(cudaMemcpyAsync(hscal + (d - dscal.p), d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+}
+void Ctx::check_flag(const int* f, const char* what) {
+  int h = 0;
+  BSGPU_CUDA(cudaMemcpyAsync(&h, f, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  if (h) {
+    BSGPU_CUDA(cudaMemsetAsync(const_cast<int*>(f), 0, sizeof(int), st));
+    throw Error(BSGPU_ERR_ARITHMETIC, what);
+  }
+}
+
+std::pair<bool, bool> Term::operator()(int iter, double R0, double R) const {
+  const double eps = 2.2204460492503131e-16 * 1000;  // IterativeSolverConfig.MachineEpsilon
+  if (mode == 2) return {iter <= max_iter, true};
+  if (mode == 3) {
+    if (iter <= 1) return {true, false};
+    if (R < R0 * reduction) return {false, true};
+    if (iter > max_iter) return {false, false};
+    return {true, false};
+  }
+  if (iter <= min_iter) return {true, false};
+  const bool ok = (mode == 0) ? (R < R0 * tol + tol) : (R < R0 * tol);
+  if (ok) return {false, true};
+  if (iter > max_iter) return {false, false};
+  if (R0 < eps || R < eps) return {false, true};
+  return {true, false};
+}
+
+namespace {
+
+template <typename T>
+void copy_vec(T* dst, const T* src, int64_t n, cudaStream_t st) {
+  if (n && dst != src) BSGPU_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+}
+
+int elt_grid(int64_t n) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 8));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// BlockJacobi (BlockJacobi.cs:68-266).  NoOfIterations = n gives n+1 updates x <- x + omega*Dinv*(b - A*x)
+// (the default termination `iter <= NoOfIterations` is tested before each update, :171-173).  Updates are fused
+// with the SpMV; the first update from a zero guess is a block-diagonal solve.  The reference's final SpMV,
+// whose residual only feeds that count-based test, is not performed.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+struct BlockJacobiT : Solver<T> {
+  const Matrix* A;
+  DBuf<T> dinv;
+  DBuf<T> tmp;
+  int updates;
+  T omega;
+  BlockJacobiT(Ctx& c, const Matrix* A64, const Matrix* AT, int iters, double om)
+      : A(AT), updates(iters + 1), omega((T)om) {
+    std::vector<int64_t> o = diag_offsets(*A64);
+    dinv.alloc(std::max<int64_t>(o.back(), 1));
+    int* err = c.flag();
+    if constexpr (sizeof(T) == 8)
+      invert_diag_blocks(*A64, dinv.p, nullptr, err, c.st);
+    else
+      invert_diag_blocks(*A64, nullptr, dinv.p, err, c.st);
+    c.check_flag(err, "BlockJacobi: singular diagonal block");
+    tmp.alloc(std::max<int64_t>(A->N, 1));
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    const int n = updates;
+    const T* src = X;
+    for (int s = 0; s < n; ++s) {
+      T* dst = ((n - 1 - s) % 2 == 0) ? X : tmp.p;
+      if (s == 0 && zero) {
+        blockdiag_apply(*A, dinv.p, omega, B, dst, c.st);
+      } else {
+        if (s == 0 && dst == X) {
+          copy_vec(tmp.p, X, A->N, c.st);
+          src = tmp.p;
+        }
+        bj_update(*A, dinv.p, omega, src, B, dst, c.st);
+      }
+      src = dst;
+    }
+    this->converged = true;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// PCG with a block-diagonal preconditioner (SoftPCG.cs:113-194; also the coarsest-level solve).  The iteration
+// runs on device scalars; its kernels are predicated on a device flag that the convergence test clears, so the
+// host launches batches of iterations and reads the state once per batch (the iterate equals that of a test
+// after every iteration).
+// scalars: s[0] rz, s[1] pq, s[2] rz_new, s[3] rr, s[4] rr0, s[5] iterations, s[6] beta, s[7] alpha
+// ---------------------------------------------------------------------------------------------------------------
+__global__ void pcg_alpha_kernel(double* s, const int* active) {
+  if (*active == 0) return;
+  s[7] = s[0] / s[1];
+}
+
+__global__ void pcg_beta_kernel(double* s, int* active, int mode, double tol, int max_iter, int min_iter) {
+  if (*active == 0) return;
+  const double rz_new = s[2], rr = s[3];
+  s[6] = rz_new / s[0];
+  s[0] = rz_new;
+  const double it = s[5] + 1.0;
+  s[5] = it;
+  const double R = sqrt(rr), R0 = sqrt(s[4]);
+  const double eps = 2.2204460492503131e-16 * 1000;
+  bool stop = false;
+  if (it > min_iter) {
+    const bool ok = (mode == 0) ? (R < R0 * tol + tol) : (R < R0 * tol);
+    if (ok || it > max_iter || R < eps || R0 < eps) stop = true;
+  }
+  if (!isfinite(rz_new) || !isfinite(rr)) stop = true;
+  if (stop) *active = 0;
+}
+
+template <typename T>
+__global__ void xpby_kernel(const T* __restrict__ z, const double* __restrict__ beta, T* __restrict__ p, int64_t n,
+                            const int* __restrict__ active) {
+  if (*active == 0) return;
+  const double b = *beta;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = (T)((double)z[i] + b * (double)p[i]);
+}
+
+__global__ void pcg_init_kernel(double* s, int* active) {
+  s[0] = s[2];  // rz
+  s[4] = s[3];  // rr0
+  s[5] = 0.0;
+  *active = 1;
+}
+
+template <typename T>
+struct PCGT : Solver<T> {
+  const Matrix* A;
+  DBuf<T> dinv;
+  DBuf<T> r, z, p, q;
+  double* s;
+  int* active;
+  Term term;
+  int batch = 8;
+  bool precond;
+  PCGT(Ctx& c, const Matrix* A64, const Matrix* AT, bool use_pc, Term t) : A(AT), term(t), precond(use_pc) {
+    const int64_t N = std::max<int64_t>(A->N, 1);
+    r.alloc(N); z.alloc(N); p.alloc(N); q.alloc(N);
+    s = c.scal(8);
+    active = c.flag();
+    if (precond) {
+      std::vector<int64_t> o = diag_offsets(*A64);
+      dinv.alloc(std::max<int64_t>(o.back(), 1));
+      int* err = c.flag();
+      if constexpr (sizeof(T) == 8)
+        invert_diag_blocks(*A64, dinv.p, nullptr, err, c.st);
+      else
+        invert_diag_blocks(*A64, nullptr, dinv.p, err, c.st);
+      c.check_flag(err, "PCG: singular diagonal block");
+    }
+  }
+  void apply_pc(Ctx& c, const T* in, T* out, const int* act) {
+    if (precond)
+      blockdiag_apply(*A, dinv.p, T(1), in, out, c.st, act);
+    else
+      copy_vec(out, in, A->N, c.st);
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    const int64_t N = A->N;
+    cudaStream_t st = c.st;
+    if (zero)
+      copy_vec(r.p, B, N, st);
+    else
+      spmv(*A, T(-1), X, T(1), B, r.p, st);
+    apply_pc(c, r.p, z.p, nullptr);
+    copy_vec(p.p, z.p, N, st);
+    {
+      const T* a[2] = {r.p, r.p};
+      const T* b[2] = {z.p, r.p};
+      dots(c.red, 2, a, b, N, s + 2, 0, st);
+    }
+    pcg_init_kernel<<<1, 1, 0, st>>>(s, active);
+    BSGPU_CHECK_LAUNCH();
+    c.fetch(s, 8);
+    const double* hs = c.hscal + (s - c.dscal.p);
+    const double R0 = std::sqrt(hs[4]);
+    this->history.assign(1, R0);
+    auto st0 = term(0, R0, R0);
+    int it = 0;
+    double R = R0;
+    if (!std::isfinite(R0)) throw Error(BSGPU_ERR_ARITHMETIC, "PCG: NaN/Inf in the initial residual");
+    if (st0.first) {
+      const int grid = elt_grid(N);
+      const T* px[1] = {p.p};
+      const T* qx[1] = {q.p};
+      while (true) {
+        for (int bi = 0; bi < batch; ++bi) {
+          spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, st, active);
+          dots(c.red, 1, px, qx, N, s + 1, 0, st, active);
+          pcg_alpha_kernel<<<1, 1, 0, st>>>(s, active);
+          BSGPU_CHECK_LAUNCH();
+          axpys(1, s + 7, nullptr, 1.0, px, X, N, st, active);
+          axpys(1, s + 7, nullptr, -1.0, qx, r.p, N, st, active);
+          apply_pc(c, r.p, z.p, active);
+          {
+            const T* a[2] = {r.p, r.p};
+            const T* b[2] = {z.p, r.p};
+            dots(c.red, 2, a, b, N, s + 2, 0, st, active);
+          }
+          pcg_beta_kernel<<<1, 1, 0, st>>>(s, active, term.mode, term.tol, term.max_iter, term.min_iter);
+          xpby_kernel<T><<<grid, 256, 0, st>>>(z.p, s + 6, p.p, N, active);
+          BSGPU_CHECK_LAUNCH();
+        }
+        int h_active = 0;
+        BSGPU_CUDA(cudaMemcpyAsync(&h_active, active, sizeof(int), cudaMemcpyDeviceToHost, st));
+        c.fetch(s, 8);
+        it = (int)hs[5];
+        R = std::sqrt(hs[3]);
+        this->history.push_back(R);
+        if (!std::isfinite(hs[3]) || !std::isfinite(hs[2])) throw Error(BSGPU_ERR_ARITHMETIC, "PCG: NaN/Inf");
+        if (!h_active) break;
+      }
+      auto fin = term(it, R0, R);
+      this->converged = fin.second;
+    } else {
+      this->converged = st0.second;
+    }
+    this->this_level_iterations = it;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// CoreOrthonormalizationProcedure (OrthonormalizationMultigrid.cs:58-445).
+// AddSol A-orthonormalises a new correction against the history.  The reference uses modified Gram-Schmidt;
+// here the projections of one sweep are computed together (classical Gram-Schmidt: one multi-dot launch, one
+// multi-axpy launch per vector set) and repeated once when the norm drops below 1/2 ("twice is enough"), which
+// restores the orthogonality MGS provides.  The reference's cancellation branch (norm <= 1e-5, up to 10
+// re-orthonormalisation sweeps, random restart) is kept as is.
+// MinimizeResidual uses RecalcResiPeriod = 1: the residual is recomputed from scratch after each update.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+struct OrthoT {
+  const Matrix* A;
+  int64_t N;
+  std::vector<DBuf<T>> Sol, Mxx;
+  int k = 0;
+  int cap = 96;
+  double* d_beta;   // [kMaxDots] projection coefficients
+  double* d_norm;   // [2]
+  double* d_alpha;  // [1]
+  bool cancellation = false;
+  OrthoT(Ctx& c, const Matrix* A_) : A(A_), N(A_->N) {
+    d_beta = c.scal(kMaxDots);
+    d_norm = c.scal(2);
+    d_alpha = c.scal(1);
+  }
+  void clear() { k = 0; }
+  bool full() const { return k >= cap; }
+  T* next_sol(Ctx& c) {
+    if ((int)Sol.size() <= k) {
+      Sol.emplace_back(std::max<int64_t>(N, 1));
+      Mxx.emplace_back(std::max<int64_t>(N, 1));
+    }
+    fill(T(0), Sol[k].p, N, c.st);
+    return Sol[k].p;
+  }
+  double norm(Ctx& c, const T* v) {
+    const T* a[1] = {v};
+    dots(c.red, 1, a, a, N, d_norm, 1, c.st);
+    return c.get(d_norm);
+  }
+  // one classical Gram-Schmidt sweep of (X, M) against the history; returns |M| afterwards
+  double cgs(Ctx& c, T* X, T* M) {
+    for (int i0 = 0; i0 < k; i0 += kMaxDots) {
+      const int kc = std::min(kMaxDots, k - i0);
+      const T* a[kMaxDots];
+      const T* b[kMaxDots];
+      for (int i = 0; i < kc; ++i) {
+        a[i] = Mxx[i0 + i].p;
+        b[i] = M;
+      }
+      dots(c.red, kc, a, b, N, d_beta, 0, c.st);
+      const T* sx[kMaxDots];
+      const T* mx[kMaxDots];
+      for (int i = 0; i < kc; ++i) {
+        sx[i] = Sol[i0 + i].p;
+        mx[i] = Mxx[i0 + i].p;
+      }
+      // NB: M is updated chunk by chunk, so later chunks project the already-updated M (block MGS)
+      axpys(kc, d_beta, nullptr, -1.0, sx, X, N, c.st);
+      axpys(kc, d_beta, nullptr, -1.0, mx, M, N, c.st);
+    }
+    return norm(c, M);
+  }
+  void random_restart(Ctx& c, T* X, T* M) {
+    fill_random(X, N, c.seed++, c.st);
+    spmv(*A, T(1), X, T(0), (const T*)nullptr, M, c.st);
+    const double nm = norm(c, M);
+    if (nm == 0 || !std::isfinite(nm))
+      throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: breakdown with a random vector");
+  }
+  // AddSol: Sol[k] holds the new correction; computes Mxx[k] and appends.
+  void add_sol(Ctx& c) {
+    T* X = Sol[k].p;
+    T* M = Mxx[k].p;
+    spmv(*A, T(1), X, T(0), (const T*)nullptr, M, c.st);
+    double nM = norm(c, M);
+    if (!std::isfinite(nM)) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: norm of matrix*solution is NaN/Inf");
+    if (nM == 0) {
+      random_restart(c, X, M);
+      nM = c.hscal[d_norm - c.dscal.p];
+    }
+    axpby(T(1.0 / nM), M, T(0), M, N, c.st);
+    axpby(T(1.0 / nM), X, T(0), X, N, c.st);
+    const int MaxOrtho = 10;
+    bool canc = false;
+    for (int jj = 0; jj <= MaxOrtho; ++jj) {
+      double nn = (k > 0) ? cgs(c, X, M) : 1.0;
+      if (k > 0 && nn > 1e-5 && nn < 0.5) nn = cgs(c, X, M);
+      if (nn <= 1e-5) {
+        canc = true;
+        if (jj < MaxOrtho) {
+          const double Xn = norm(c, X);
+          if (Xn < 1e-200 || jj == MaxOrtho - 1) {
+            random_restart(c, X, M);
+          } else {
+            axpby(T(1.0 / Xn), X, T(0), X, N, c.st);
+            spmv(*A, T(1), X, T(0), (const T*)nullptr, M, c.st);
+            if (norm(c, M) == 0) random_restart(c, X, M);
+          }
+          axpby(T(1.0 / nn), M, T(0), M, N, c.st);
+          axpby(T(1.0 / nn), X, T(0), X, N, c.st);
+        } else {
+          throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: numerical breakdown");
+        }
+      } else {
+        if (nn != 1.0) {
+          axpby(T(1.0 / nn), M, T(0), M, N, c.st);
+          axpby(T(1.0 / nn), X, T(0), X, N, c.st);
+        }
+        break;
+      }
+    }
+    cancellation = canc;
+    ++k;
+  }
+  // MinimizeResidual: X += alpha*Sol[k-1], alpha = <Mxx[k-1], Res0>; Res = B - A*X; returns |Res|.
+  double minimize(Ctx& c, T* X, const T* B, const T* Res0, T* Res, double oldN) {
+    const int i = k - 1;
+    const T* a[1] = {Mxx[i].p};
+    const T* b[1] = {Res0};
+    dots(c.red, 1, a, b, N, d_alpha, 0, c.st);
+    const T* sx[1] = {Sol[i].p};
+    axpys(1, d_alpha, nullptr, 1.0, sx, X, N, c.st);
+    spmv(*A, T(-1), X, T(1), B, Res, c.st);
+    const double rn = norm(c, Res);
+    if (!std::isfinite(rn)) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: residual is NaN/Inf");
+    const double tol = std::max(std::max(rn, oldN) * 0.2, 1.0e-7);
+    if (rn > oldN + tol) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: residual increase");
+    return rn;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// OrthonormalizationMultigrid.Solve (OrthonormalizationMultigrid.cs:797-1104) as configured by PmgConfig
+// (PmgConfig.cs:80-245): no pre-smoother, m_omega = 1, coarse correction on the same level through
+// GridAndDegRestriction (CoarseOnLowerLevel = false), NoOfPostSmootherSweeps post-smoother calls, each followed
+// by orthonormalisation and residual minimisation.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+struct OrthoMGT : Solver<T> {
+  const Matrix* A;
+  int64_t N;
+  std::unique_ptr<Solver<T>> coarse, post;
+  int sweeps = 10;
+  Term term;
+  OrthoT<T> ortho;
+  DBuf<T> Res0, Res;
+  OrthoMGT(Ctx& c, const Matrix* A_, Term t) : A(A_), N(A_->N), term(t), ortho(c, A_) {
+    Res0.alloc(std::max<int64_t>(N, 1));
+    Res.alloc(std::max<int64_t>(N, 1));
+  }
+  int nested() const override {
+    int s = 0;
+    if (coarse) s += coarse->this_level_iterations + coarse->nested();
+    if (post) s += post->this_level_iterations + post->nested();
+    return s;
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    if (zero)
+      copy_vec(Res0.p, B, N, c.st);
+    else
+      spmv(*A, T(-1), X, T(1), B, Res0.p, c.st);
+    copy_vec(Res.p, Res0.p, N, c.st);
+    const double r0 = ortho.norm(c, Res0.p);
+    double rn = r0;
+    this->history.assign(1, r0);
+    ortho.clear();
+    this->converged = false;
+    for (int iIter = 1;; ++iIter) {
+      auto st = term(iIter, r0, rn);
+      if (!st.first) {
+        this->converged = st.second;
+        break;
+      }
+      if (ortho.full() ) {
+        // history capacity reached: restart the minimisation from the current iterate
+        copy_vec(Res0.p, Res.p, N, c.st);
+        ortho.clear();
+      }
+      if (coarse) {
+        T* vl = ortho.next_sol(c);
+        coarse->solve(c, vl, Res.p, true);
+        ortho.add_sol(c);
+        rn = ortho.minimize(c, X, B, Res0.p, Res.p, rn);
+        st = term(iIter, r0, rn);
+        if (!st.first) {
+          this->converged = st.second;
+          break;
+        }
+      }
+      bool termPost = false;
+      if (post) {
+        for (int g = 0; g < sweeps; ++g) {
+          if (ortho.full()) break;
+          T* pc = ortho.next_sol(c);
+          post->solve(c, pc, Res.p, true);
+          ortho.add_sol(c);
+          rn = ortho.minimize(c, X, B, Res0.p, Res.p, rn);
+          st = term(iIter, r0, rn);
+          if (!st.first) {
+            this->converged = st.second;
+            termPost = true;
+            break;
+          }
+          if (ortho.cancellation) break;
+        }
+      }
+      if (termPost) break;
+      this->this_level_iterations++;
+      this->history.push_back(rn);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// GridAndDegRestriction.Solve (GridAndDegRestriction.cs:379-439): solve on the leading modes, add back.
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+struct GridAndDegT : Solver<T> {
+  const Matrix* A;    // level operator
+  const Matrix* sub;  // restricted operator (same precision)
+  int keep;
+  std::unique_ptr<Solver<T>> lower;
+  DBuf<T> xLo, bLo;
+  DBuf<int64_t> map;  // sub -> full index (non-uniform blocks only)
+  double* d_norm;
+  GridAndDegT(Ctx& c, const Matrix* A_, const Matrix* sub_, int keep_) : A(A_), sub(sub_), keep(keep_) {
+    xLo.alloc(std::max<int64_t>(sub->N, 1));
+    bLo.alloc(std::max<int64_t>(sub->N, 1));
+    d_norm = c.scal(1);
+    if (!A->uniform) {
+      std::vector<int64_t> m(sub->N);
+      for (int64_t i = 0; i < A->nb; ++i)
+        for (int s = 0; s < A->h_nspc[i]; ++s)
+          for (int q = 0; q < keep; ++q) m[sub->h_i0[i] + s * keep + q] = A->h_i0[i] + s * A->Np + q;
+      map.alloc(std::max<int64_t>(sub->N, 1));
+      if (sub->N) BSGPU_CUDA(cudaMemcpy(map.p, m.data(), sub->N * 8, cudaMemcpyHostToDevice));
+    }
+  }
+  int nested() const override { return lower ? lower->this_level_iterations + lower->nested() : 0; }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    restrict_gather(B, bLo.p, sub->N, A->Np, keep, map.p, c.st);
+    const T* a[1] = {bLo.p};
+    dots(c.red, 1, a, a, sub->N, d_norm, 1, c.st);
+    if (!(c.get(d_norm) > 0)) {
+      this->converged = true;
+      return;
+    }
+    if (zero)
+      fill(T(0), xLo.p, sub->N, c.st);
+    else
+      restrict_gather(X, xLo.p, sub->N, A->Np, keep, map.p, c.st);
+    lower->solve(c, xLo.p, bLo.p, zero);
+    this->converged = lower->converged;
+    restrict_scatter_add(xLo.p, X, sub->N, A->Np, keep, map.p, c.st);
+  }
+};
+
+// FP64 interface around an FP32 solver (mixed-precision preconditioner).
+struct MixedAdapter : Solver<double> {
+  std::unique_ptr<Solver<float>> inner;
+  DBuf<float> x32, b32;
+  int64_t N;
+  explicit MixedAdapter(int64_t n) : N(n) {
+    x32.alloc(std::max<int64_t>(n, 1));
+    b32.alloc(std::max<int64_t>(n, 1));
+  }
+  int nested() const override { return inner->this_level_iterations + inner->nested(); }
+  void solve(Ctx& c, double* X, const double* B, bool zero) override {
+    convert(B, b32.p, N, c.st);
+    if (zero)
+      fill(0.0f, x32.p, N, c.st);
+    else
+      convert(X, x32.p, N, c.st);
+    inner->solve(c, x32.p, b32.p, zero);
+    convert(x32.p, X, N, c.st);
+    this->converged = inner->converged;
+    this->this_level_iterations = inner->this_level_iterations;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// FlexGMRES (FlexGMRES.cs:144-277), Saad-1993 FGMRES(m): the minimal-residual combination of the preconditioned
+// vectors Z_j is formed from the least-squares solution of the Hessenberg system (Givens rotations, the dgelsy
+// solution for full-rank H).  The reference overwrites that solution with (beta, 0, ..., 0) at :259-260, which
+// reduces it to preconditioned Richardson; this implementation does not.  The implicit residual |g_{j+1}| is
+// tested after every Arnoldi step; the true residual is recomputed at every restart.  Arnoldi uses classical
+// Gram-Schmidt applied twice (one multi-dot and one multi-axpy launch per sweep) instead of MGS.
+// ---------------------------------------------------------------------------------------------------------------
+struct FlexGMRES : Solver<double> {
+  const Matrix* A;
+  int64_t N;
+  int m;
+  Term term;
+  std::unique_ptr<Solver<double>> pc;
+  std::vector<DBuf<double>> V, Z;
+  DBuf<double> R0;
+  double* d_h;     // [2*(m+1)] projections of both sweeps
+  double* d_norm;  // [1]
+  FlexGMRES(Ctx& c, const Matrix* A_, int m_, Term t) : A(A_), N(A_->N), m(m_), term(t) {
+    for (int j = 0; j <= m; ++j) V.emplace_back(std::max<int64_t>(N, 1));
+    for (int j = 0; j < m; ++j) Z.emplace_back(std::max<int64_t>(N, 1));
+    R0.alloc(std::max<int64_t>(N, 1));
+    d_h = c.scal(2 * (m + 1));
+    d_norm = c.scal(1);
+  }
+  int nested() const override { return pc ? pc->this_level_iterations + pc->nested() : 0; }
+  double norm(Ctx& c, const double* v) {
+    const double* a[1] = {v};
+    dots(c.red, 1, a, a, N, d_norm, 1, c.st);
+    return c.get(d_norm);
+  }
+  // W -= sum_i h_i V_i for i <= j; projections into d_h[off..off+j]
+  void project(Ctx& c, int j, double* W, int off) {
+    for (int i0 = 0; i0 <= j; i0 += kMaxDots) {
+      const int kc = std::min(kMaxDots, j + 1 - i0);
+      const double* a[kMaxDots];
+      const double* b[kMaxDots];
+      for (int i = 0; i < kc; ++i) {
+        a[i] = V[i0 + i].p;
+        b[i] = W;
+      }
+      dots(c.red, kc, a, b, N, d_h + off + i0, 0, c.st);
+    }
+    std::vector<const double*> vx(j + 1);
+    for (int i = 0; i <= j; ++i) vx[i] = V[i].p;
+    axpys(j + 1, d_h + off, nullptr, -1.0, vx.data(), W, N, c.st);
+  }
+  void solve(Ctx& c, double* X, const double* B, bool zero) override {
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    int iIter = 0;
+    double r0 = 0;
+    this->history.clear();
+    bool first = true;
+    while (true) {
+      if (first && zero)
+        copy_vec(R0.p, B, N, c.st);
+      else
+        spmv(*A, -1.0, X, 1.0, B, R0.p, c.st);
+      first = false;
+      const double r = norm(c, R0.p);
+      if (!std::isfinite(r)) throw Error(BSGPU_ERR_ARITHMETIC, "FlexGMRES: residual is NaN/Inf");
+      if (iIter == 0) r0 = r;
+      this->history.push_back(r);
+      auto st = term(iIter, r0, r);
+      if (!st.first || st.second) {
+        this->converged = st.second;
+        this->this_level_iterations = iIter;
+        return;
+      }
+      axpby(1.0 / r, R0.p, 0.0, V[0].p, N, c.st);
+      std::fill(g.begin(), g.end(), 0.0);
+      g[0] = r;
+      int j;
+      for (j = 0; j < m; ++j) {
+        fill(0.0, Z[j].p, N, c.st);
+        pc->solve(c, Z[j].p, V[j].p, true);
+        iIter++;
+        double* W = V[j + 1].p;
+        spmv(*A, 1.0, Z[j].p, 0.0, (const double*)nullptr, W, c.st);
+        project(c, j, W, 0);
+        project(c, j, W, m + 1);
+        const double* a[1] = {W};
+        dots(c.red, 1, a, a, N, d_norm, 1, c.st);
+        c.fetch(d_h, 2 * (m + 1) + 1);
+        const double* hh = c.hscal + (d_h - c.dscal.p);
+        const double wn = hh[2 * (m + 1)];
+        if (!std::isfinite(wn)) throw Error(BSGPU_ERR_ARITHMETIC, "FlexGMRES: Arnoldi vector is NaN/Inf");
+        for (int i = 0; i <= j; ++i) H[i * m + j] = hh[i] + hh[m + 1 + i];
+        H[(j + 1) * m + j] = wn;
+        if (wn > 0) axpby(1.0 / wn, W, 0.0, W, N, c.st);
+        for (int i = 0; i < j; ++i) {
+          const double a0 = H[i * m + j], b0 = H[(i + 1) * m + j];
+          H[i * m + j] = cs[i] * a0 + sn[i] * b0;
+          H[(i + 1) * m + j] = -sn[i] * a0 + cs[i] * b0;
+        }
+        const double a0 = H[j * m + j], b0 = H[(j + 1) * m + j];
+        const double den = std::hypot(a0, b0);
+        cs[j] = a0 / den;
+        sn[j] = b0 / den;
+        H[j * m + j] = den;
+        H[(j + 1) * m + j] = 0.0;
+        g[j + 1] = -sn[j] * g[j];
+        g[j] = cs[j] * g[j];
+        const double est = std::fabs(g[j + 1]);
+        this->history.push_back(est);
+        auto st2 = term(iIter, r0, est);
+        if (!st2.first || st2.second || wn == 0.0) {
+          ++j;
+          break;
+        }
+      }
+      const int kk = j;
+      for (int i = kk - 1; i >= 0; --i) {
+        double s = g[i];
+        for (int q = i + 1; q < kk; ++q) s -= H[i * m + q] * y[q];
+        y[i] = s / H[i * m + i];
+      }
+      std::vector<const double*> zx(kk);
+      for (int i = 0; i < kk; ++i) zx[i] = Z[i].p;
+      axpys(kk, nullptr, y.data(), 1.0, zx.data(), X, N, c.st);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// tree construction (PmgConfig.CreateInstanceImpl__Kummer, PmgConfig.cs:80-245, with UseILU = false)
+// ---------------------------------------------------------------------------------------------------------------
+template <typename T>
+const Matrix* level_matrix(Tree& t, const Matrix* A64) {
+  if constexpr (sizeof(T) == 8) {
+    return A64;
+  } else {
+    t.owned.emplace_back(matrix_to_single(*A64, t.ctx->st));
+    return t.owned.back().get();
+  }
+}
+
+// A64: FP64 level operator (factorisations are computed from it); AT: the same operator in the precision T the
+// level runs in (AT == A64 for T = double).
+template <typename T>
+std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix* AT, int level, const Term& top) {
+  const bsgpu_solver_config& cfg = t.cfg;
+  Ctx& c = *t.ctx;
+  if (level == cfg.n_levels - 1) {
+    require(cfg.coarse_kind == BSGPU_COARSE_PCG, "only the PCG coarse solve is available", BSGPU_ERR_UNSUPPORTED);
+    Term ct;
+    ct.mode = 1;
+    ct.tol = cfg.coarse_tol;
+    ct.max_iter = cfg.coarse_max_iter;
+    ct.min_iter = 0;
+    return std::make_unique<PCGT<T>>(c, A64, AT, true, ct);
+  }
+  Term lt = top;
+  if (level > 0) {
+    lt.mode = 3;
+    lt.reduction = cfg.sub_reduction;
+    lt.max_iter = cfg.sub_max_iter;
+  }
+  auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
+  omg->sweeps = cfg.post_sweeps;
+  omg->post = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
+  const int keep = cfg.level_keep[level + 1];
+  t.owned.emplace_back(matrix_restrict(*A64, keep, c.st));
+  const Matrix* sub64 = t.owned.back().get();
+  const Matrix* subT = level_matrix<T>(t, sub64);
+  auto gr = std::make_unique<GridAndDegT<T>>(c, AT, subT, keep);
+  gr->lower = build_level<T>(t, sub64, subT, level + 1, top);
+  omg->coarse = std::move(gr);
+  return omg;
+}
+
+}  // namespace
+
+Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg) {
+  require(!A->single, "the solver operator must be FP64");
+  require(cfg.n_levels >= 1 && cfg.n_levels <= 8, "n_levels must be in 1..8");
+  auto t = std::make_unique<Tree>();
+  t->ctx = std::make_unique<Ctx>();
+  t->A = A;
+  t->cfg = cfg;
+  Term top;
+  top.mode = cfg.termination == BSGPU_TERM_RELATIVE ? 1 : 0;
+  top.tol = cfg.tol;
+  top.max_iter = cfg.max_iter;
+  top.min_iter = cfg.min_iter;
+  if (cfg.solver != BSGPU_SOLVER_SOFTPCG && cfg.solver != BSGPU_SOLVER_BLOCKJACOBI) {
+    require(cfg.level_keep[0] == A->Np, "level_keep[0] must equal Np");
+    for (int l = 1; l < cfg.n_levels; ++l)
+      require(cfg.level_keep[l] >= 1 && cfg.level_keep[l] < cfg.level_keep[l - 1], "level_keep must decrease");
+  }
+  const bool mixed = cfg.precision == BSGPU_PRECISION_MIXED;
+  switch (cfg.solver) {
+    case BSGPU_SOLVER_SOFTPCG: {
+      require(!mixed, "mixed precision is available for the FGMRES preconditioner", BSGPU_ERR_UNSUPPORTED);
+      t->top = std::make_unique<PCGT<double>>(*t->ctx, A, A, cfg.bj_iters >= 0, top);
+      break;
+    }
+    case BSGPU_SOLVER_BLOCKJACOBI:
+      t->top = std::make_unique<BlockJacobiT<double>>(*t->ctx, A, A, cfg.bj_iters, cfg.bj_omega);
+      break;
+    case BSGPU_SOLVER_ORTHOMG:
+      require(!mixed, "mixed precision is available for the FGMRES preconditioner", BSGPU_ERR_UNSUPPORTED);
+      t->top = build_level<double>(*t, A, A, 0, top);
+      break;
+    case BSGPU_SOLVER_FGMRES_PMG: {
+      require(cfg.max_krylov >= 1 && cfg.max_krylov <= 256, "max_krylov must be in 1..256");
+      Term one;
+      one.mode = 2;
+      one.max_iter = 1;
+      auto f = std::make_unique<FlexGMRES>(*t->ctx, A, cfg.max_krylov, top);
+      if (mixed) {
+        auto ad = std::make_unique<MixedAdapter>(A->N);
+        ad->inner = build_level<float>(*t, A, level_matrix<float>(*t, A), 0, one);
+        f->pc = std::move(ad);
+      } else {
+        f->pc = build_level<double>(*t, A, A, 0, one);
+      }
+      t->top = std::move(f);
+      break;
+    }
+    default:
+      throw Error(BSGPU_ERR_ARGUMENT, "unknown solver kind");
+  }
+  BSGPU_CUDA(cudaStreamSynchronize(t->ctx->st));
+  return t.release();
+}
+
+}  // namespace bsgpu

@@ -1,0 +1,72 @@
+// Solver tree of the hot path: BlockJacobi, GridAndDegRestriction, OrthonormalizationMultigrid (p-multigrid),
+// FlexGMRES, SoftPCG and the coarsest-level solve.  Host C++ drives the kernels of matrix.cu / blas1.cu on one
+// CUDA stream; scalars (norms, projection coefficients) stay in device memory and the host reads back only the
+// values its control flow branches on.
+#pragma once
+#include <memory>
+
+#include "blas1.cuh"
+#include "blockops.cuh"
+#include "matrix.cuh"
+
+namespace bsgpu {
+
+// Per-solver-tree execution context.
+struct Ctx {
+  cudaStream_t st = nullptr;
+  ReduceScratch red;
+  DBuf<double> dscal;   // device scalars
+  double* hscal = nullptr;  // pinned mirror
+  DBuf<int> dflag;      // device error flags
+  int nscal = 0, nflag = 0;
+  int scal_cap = 4096;
+  uint64_t seed = 12345;
+  Ctx();
+  ~Ctx();
+  double* scal(int n);  // allocate n device scalars
+  int* flag();
+  // copy device scalars to the host mirror and wait
+  void fetch(const double* d, int n);
+  double get(const double* d) {
+    fetch(d, 1);
+    return hscal[d - dscal.p];
+  }
+  void check_flag(const int* f, const char* what);
+};
+
+template <typename T>
+struct Solver {
+  virtual ~Solver() {}
+  // X: initial guess in, solution out (device); B: right-hand side (device).  zero_guess: X is known to be 0.
+  virtual void solve(Ctx& c, T* X, const T* B, bool zero_guess) = 0;
+  virtual int nested() const { return 0; }
+  int this_level_iterations = 0;
+  bool converged = false;
+  std::vector<double> history;
+};
+
+// Termination criteria (IterativeSolverConfig.cs:48-62, PmgConfig.cs:202-215).
+struct Term {
+  int mode = 0;  // 0: R < R0*tol + tol, 1: R < R0*tol, 2: fixed iteration count, 3: sub-level (reduction)
+  double tol = 1e-10;
+  int max_iter = 300, min_iter = 1;
+  double reduction = 0.1;
+  std::pair<bool, bool> operator()(int iter, double R0, double R) const;
+};
+
+struct TreeConfig {
+  bsgpu_solver_config cfg;
+};
+
+// Builds the solver tree for `cfg` on the (transformed) operator A (FP64).  For BSGPU_PRECISION_MIXED the
+// preconditioner runs on FP32 copies of the level matrices.
+struct Tree {
+  std::unique_ptr<Ctx> ctx;
+  std::vector<std::unique_ptr<Matrix>> owned;
+  std::unique_ptr<Solver<double>> top;
+  const Matrix* A = nullptr;
+  bsgpu_solver_config cfg{};
+};
+Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg);
+
+}  // namespace bsgpu

@@ -1,0 +1,342 @@
+"""Host-side mirror of the BoSSS solver-path API over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference:
+
+* ``BlockMsrMatrix`` -- ``src/L1-platform/BoSSS.Platform/BlockMsrMatrix.cs:191``; ``SpMV(alpha, a, beta, acc)``
+  (``:2970``) raises ``ValueError`` (the reference's ``ArgumentException``) on length mismatch or aliasing.
+* ``MultigridOperator`` -- ``src/L3-solution/BoSSS.Solution.AdvancedSolvers/MultigridOperator.cs:37`` with the
+  ``DiagBlockEquilib`` change of basis (``MultigridOperator_ChangeOfBasis.cs:624``).
+* Solver configurations implement ``ISolverFactory.CreateInstance(MultigridOperator)``
+  (``ISmootherTemplate.cs:136-152``): ``FGMRESConfig`` (``FlexGMRES.cs:35``), ``PmgConfig`` (``PmgConfig.cs:80``),
+  ``SoftPCGConfig`` (``SoftPCG.cs:37``), ``BlockJacobiConfig`` (``BlockJacobi.cs:35``).  The returned solver
+  implements ``ISolverSmootherTemplate`` (``ISmootherTemplate.cs:29-83``): ``Solve(X, B)`` with X the initial
+  guess in and the solution out, ``ThisLevelIterations``, ``IterationsInNested``, ``Converged``, ``ResetStat``,
+  ``Dispose``.  Non-convergence is not an exception; NaN/Inf or breakdown raise ``ArithmeticError``.
+
+Vectors may be numpy arrays (host; copied to and from the device by the library) or CUDA torch tensors
+(device-resident; no copies).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import native as nat
+
+
+def _is_device(a) -> bool:
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+class BlockMsrMatrix:
+    """Device-resident block-sparse matrix with dense Np x Np (or nspc*Np) blocks."""
+
+    def __init__(self, handle: C.c_void_p, owner: bool = True, single: bool = False):
+        self._h = handle
+        self._owner = owner
+        self.single = single
+        n, nb, nnzb, Np = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int32()
+        nat.check(nat.lib().bsgpu_matrix_get_info(self._h, C.byref(n), C.byref(nb), C.byref(nnzb), C.byref(Np)))
+        self.N, self.NoOfBlocks, self.nnzb, self.Np = n.value, nb.value, nnzb.value, Np.value
+
+    @classmethod
+    def from_bsr(cls, Np: int, row_ptr, col_idx, values, nspc=None) -> "BlockMsrMatrix":
+        """values: row-major blocks concatenated in block-CSR order (numpy on the host or CUDA tensors)."""
+        dev = _is_device(values)
+        if dev:
+            import torch
+            row_ptr = row_ptr.to(torch.int64).contiguous()
+            col_idx = col_idx.to(torch.int32).contiguous()
+            values = values.to(torch.float64).contiguous()
+            nspc = None if nspc is None else nspc.to(torch.int32).contiguous()
+        else:
+            row_ptr = np.ascontiguousarray(row_ptr, np.int64)
+            col_idx = np.ascontiguousarray(col_idx, np.int32)
+            values = np.ascontiguousarray(values, np.float64)
+            nspc = None if nspc is None else np.ascontiguousarray(nspc, np.int32)
+        nb = (row_ptr.shape[0] if dev else len(row_ptr)) - 1
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_matrix_create(
+            C.byref(h), nb, int(Np), None if nspc is None else nat.ptr(nspc), nat.ptr(row_ptr), nat.ptr(col_idx),
+            nat.ptr(values), nat.DEVICE_POINTERS if dev else nat.HOST_POINTERS))
+        return cls(h)
+
+    @classmethod
+    def from_system(cls, s) -> "BlockMsrMatrix":
+        return cls.from_bsr(s.Np, s.row_ptr, s.col_idx, s.values, getattr(s, "nspc", None))
+
+    # --- reference API -------------------------------------------------------------------------------------------
+    def SpMV(self, alpha: float, a, beta: float, acc):
+        """acc = alpha*A*a + beta*acc (BlockMsrMatrix.SpMV)."""
+        if a is acc:
+            raise ValueError("In-Place computation is not supported.")
+        na = a.numel() if _is_device(a) else len(a)
+        nacc = acc.numel() if _is_device(acc) else len(acc)
+        if na != self.N:
+            raise ValueError("Mismatch in number of columns.")
+        if nacc != self.N:
+            raise ValueError("Mismatch in number of rows.")
+        if _is_device(a) != _is_device(acc):
+            raise ValueError("a and acc must both live on the host or both on the device")
+        if self.single:
+            if not _is_device(a):
+                raise ValueError("single-precision matrices take device vectors")
+            nat.check(nat.lib().bsgpu_matrix_spmv_device_f32(self._h, float(alpha), nat.ptr(a), float(beta),
+                                                             nat.ptr(acc), None))
+            return acc
+        if _is_device(a):
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+            nat.check(nat.lib().bsgpu_matrix_spmv_device(self._h, float(alpha), nat.ptr(a), float(beta), nat.ptr(acc),
+                                                         C.c_void_p(stream)))
+        else:
+            if acc.dtype != np.float64 or not acc.flags.c_contiguous:
+                raise ValueError("acc must be a contiguous float64 array")
+            a = np.ascontiguousarray(a, np.float64)
+            nat.check(nat.lib().bsgpu_matrix_spmv(self._h, float(alpha), nat.ptr(a), float(beta), nat.ptr(acc)))
+        return acc
+
+    def ToSingle(self) -> "BlockMsrMatrix":
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_matrix_create_single(self._h, C.byref(h)))
+        return BlockMsrMatrix(h, single=True)
+
+    def Restrict(self, keep: int) -> "BlockMsrMatrix":
+        """Sub-matrix of the leading ``keep`` modes per species (GridAndDegRestriction's coarse operator)."""
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_matrix_restrict(self._h, int(keep), C.byref(h)))
+        return BlockMsrMatrix(h)
+
+    def read_values(self, nvals: Optional[int] = None) -> np.ndarray:
+        """All blocks, row-major, in block-CSR order (the layout of ReadBlock).
+
+        ``nvals`` (the total number of block entries) is needed for blocks of uneven size."""
+        if nvals is None:
+            if self.N != self.NoOfBlocks * self.Np:
+                raise ValueError("uneven block sizes: pass nvals")
+            nvals = self.nnzb * self.Np * self.Np
+        out = np.empty(nvals)
+        nat.check(nat.lib().bsgpu_matrix_read_values(self._h, nat.ptr(out), nat.HOST_POINTERS))
+        return out
+
+    def Dispose(self):
+        if self._h is not None and self._owner:
+            nat.lib().bsgpu_matrix_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.Dispose()
+        except Exception:
+            pass
+
+
+class MultigridOperator:
+    """Operator as seen by the solvers: L*A*L^T with L from SymmInv of each diagonal block."""
+
+    Eye, DiagBlockEquilib = nat.COB_EYE, nat.COB_DIAG_BLOCK_EQUILIB
+
+    def __init__(self, A: BlockMsrMatrix, mode: int = nat.COB_DIAG_BLOCK_EQUILIB):
+        self.BaseMatrix = A
+        self.mode = mode
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_mgop_create(C.byref(h), A._h, int(mode)))
+        self._h = h
+        oh = C.c_void_p()
+        nat.check(nat.lib().bsgpu_mgop_get_operator(self._h, C.byref(oh)))
+        self.OperatorMatrix = BlockMsrMatrix(oh, owner=False)
+
+    def LeftChangeOfBasis(self, total_len: int) -> np.ndarray:
+        out = np.empty(total_len)
+        nat.check(nat.lib().bsgpu_mgop_read_left_cob(self._h, nat.ptr(out)))
+        return out
+
+    def Dispose(self):
+        if self._h is not None:
+            nat.lib().bsgpu_mgop_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.Dispose()
+        except Exception:
+            pass
+
+
+@dataclass
+class IterativeSolverConfig:
+    """IterativeSolverConfig.cs:19-62.  termination: 'default' (R < R0*tol + tol) or 'relative' (R < R0*tol)."""
+    ConvergenceCriterion: float = 1e-10
+    MaxSolverIterations: int = 300
+    MinSolverIterations: int = 1
+    termination: str = "default"
+
+    def _base(self) -> nat.SolverConfig:
+        c = nat.SolverConfig()
+        nat.check(nat.lib().bsgpu_solver_config_default(C.byref(c)))
+        c.tol = self.ConvergenceCriterion
+        c.max_iter = self.MaxSolverIterations
+        c.min_iter = self.MinSolverIterations
+        c.termination = nat.TERM_RELATIVE if self.termination == "relative" else nat.TERM_DEFAULT
+        return c
+
+    def CreateInstance(self, op: MultigridOperator) -> "GpuSolver":
+        return GpuSolver(op, self._config())
+
+
+@dataclass
+class PmgConfig(IterativeSolverConfig):
+    """PmgConfig.CreateInstanceImpl__Kummer with UseILU = false (block-Jacobi post-smoother on every level).
+
+    ``DegreeHierarchy``: modes per species kept on each level, finest first (e.g. (20, 10, 4) for p = 3 -> 2 -> 1
+    in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative).
+    """
+    DegreeHierarchy: tuple = (20, 10, 4)
+    NoOfPostSmootherSweeps: int = 10
+    BlockJacobiIterations: int = 1
+    BlockJacobiOmega: float = 1.0
+    CoarseTolerance: float = 1e-3
+    CoarseMaxIterations: int = 2000
+    SubLevelMaxIterations: int = 100
+    SubLevelReduction: float = 0.1
+    UseILU: bool = False
+
+    def _fill(self, c):
+        if self.UseILU:
+            raise NotImplementedError("CellILU smoothing is not available; set UseILU = False")
+        c.n_levels = len(self.DegreeHierarchy)
+        for i, k in enumerate(self.DegreeHierarchy):
+            c.level_keep[i] = int(k)
+        c.post_sweeps = self.NoOfPostSmootherSweeps
+        c.bj_iters = self.BlockJacobiIterations
+        c.bj_omega = self.BlockJacobiOmega
+        c.coarse_kind = nat.COARSE_PCG
+        c.coarse_tol = self.CoarseTolerance
+        c.coarse_max_iter = self.CoarseMaxIterations
+        c.sub_max_iter = self.SubLevelMaxIterations
+        c.sub_reduction = self.SubLevelReduction
+
+    def _config(self):
+        c = self._base()
+        c.solver = nat.SOLVER_ORTHOMG
+        self._fill(c)
+        return c
+
+
+@dataclass
+class FGMRESConfig(IterativeSolverConfig):
+    """FGMRESConfig (FlexGMRES.cs:35) with one p-multigrid V-cycle (a PmgConfig) as preconditioner.
+
+    ``MixedPrecision``: the preconditioner runs in FP32 (matrices, block-Jacobi factors and vectors); the outer
+    residual, the Arnoldi process and the solution update stay FP64.
+    """
+    MaxKrylovDim: int = 30
+    Preconditioners: List[PmgConfig] = field(default_factory=lambda: [PmgConfig()])
+    MixedPrecision: bool = False
+
+    def _config(self):
+        if len(self.Preconditioners) != 1:
+            raise NotImplementedError("exactly one PmgConfig preconditioner is supported")
+        c = self._base()
+        c.solver = nat.SOLVER_FGMRES_PMG
+        c.max_krylov = self.MaxKrylovDim
+        self.Preconditioners[0]._fill(c)
+        c.precision = nat.PRECISION_MIXED if self.MixedPrecision else nat.PRECISION_FP64
+        return c
+
+
+@dataclass
+class SoftPCGConfig(IterativeSolverConfig):
+    """SoftPCG (SoftPCG.cs:37) preconditioned by the inverse block diagonal (``BlockJacobiPrecond``)."""
+    BlockJacobiPrecond: bool = True
+
+    def _config(self):
+        c = self._base()
+        c.solver = nat.SOLVER_SOFTPCG
+        c.bj_iters = 0 if self.BlockJacobiPrecond else -1
+        return c
+
+
+@dataclass
+class BlockJacobiConfig:
+    """BlockJacobi (BlockJacobi.cs:35): NoOfIterations, omega."""
+    NoOfIterations: int = 1
+    omega: float = 1.0
+
+    def CreateInstance(self, op: MultigridOperator) -> "GpuSolver":
+        c = nat.SolverConfig()
+        nat.check(nat.lib().bsgpu_solver_config_default(C.byref(c)))
+        c.solver = nat.SOLVER_BLOCKJACOBI
+        c.bj_iters = self.NoOfIterations
+        c.bj_omega = self.omega
+        return GpuSolver(op, c)
+
+
+class GpuSolver:
+    """ISolverSmootherTemplate backed by a bsgpu solver handle."""
+
+    def __init__(self, op: MultigridOperator, cfg: nat.SolverConfig):
+        self.op = op
+        self.cfg = cfg
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_solver_create(C.byref(h), op._h, C.byref(cfg)))
+        self._h = h
+        self.stats = nat.SolveStats()
+
+    def Solve(self, X, B):
+        """X: initial guess in, solution out; B: right-hand side (original basis)."""
+        N = self.op.BaseMatrix.N
+        nx = X.numel() if _is_device(X) else len(X)
+        nb = B.numel() if _is_device(B) else len(B)
+        if nx != N:
+            raise ValueError("Wrong length of unknowns vector.")
+        if nb != N:
+            raise ValueError("Wrong length of RHS vector.")
+        if _is_device(X):
+            nat.check(nat.lib().bsgpu_solver_solve_device(self._h, nat.ptr(X), nat.ptr(B), C.byref(self.stats)))
+        else:
+            if X.dtype != np.float64 or not X.flags.c_contiguous:
+                raise ValueError("X must be a contiguous float64 array")
+            B = np.ascontiguousarray(B, np.float64)
+            nat.check(nat.lib().bsgpu_solver_solve(self._h, nat.ptr(X), nat.ptr(B), C.byref(self.stats)))
+        return X
+
+    @property
+    def ThisLevelIterations(self) -> int:
+        return self.stats.iterations
+
+    @property
+    def IterationsInNested(self) -> int:
+        return self.stats.nested
+
+    @property
+    def Converged(self) -> bool:
+        return bool(self.stats.converged)
+
+    @property
+    def SolveSeconds(self) -> float:
+        return self.stats.seconds
+
+    def ResetStat(self):
+        self.stats = nat.SolveStats()
+
+    def History(self) -> np.ndarray:
+        n = C.c_int32()
+        nat.check(nat.lib().bsgpu_solver_get_history(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 1))
+        nat.check(nat.lib().bsgpu_solver_get_history(self._h, nat.ptr(out), n.value, C.byref(n)))
+        return out[:n.value]
+
+    def Dispose(self):
+        if self._h is not None:
+            nat.lib().bsgpu_solver_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.Dispose()
+        except Exception:
+            pass

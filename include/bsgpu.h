@@ -1,0 +1,156 @@
+/*
+ * bsgpu -- B200-native (sm_100a) library for the BoSSS linear-solver hot path.
+ *
+ * C ABI for P/Invoke (C#), ctypes (Python) or plain C/C++.  All handles are opaque; every function returns an
+ * int status (BSGPU_OK = 0).  Host arrays are plain pointers + sizes; functions ending in _device take device
+ * pointers and an optional cudaStream_t passed as void* (NULL = the handle's own stream).
+ *
+ * Reference interfaces replaced (paths relative to the BoSSS source tree):
+ *   BlockMsrMatrix            src/L1-platform/BoSSS.Platform/BlockMsrMatrix.cs:191 (SpMV :2970, ReadBlock :1743)
+ *   MultigridOperator         src/L3-solution/BoSSS.Solution.AdvancedSolvers/MultigridOperator.cs:37
+ *                             (change of basis :650-700, UseSolver :1213-1262)
+ *   ISolverSmootherTemplate   src/L3-solution/BoSSS.Solution.AdvancedSolvers/ISmootherTemplate.cs:29-83
+ *   ISolverFactory            ISmootherTemplate.cs:136-152 (configs: PmgConfig.cs:80, FlexGMRES.cs:35,
+ *                             SoftPCG.cs:37, BlockJacobi.cs:35)
+ *   native binding precedent  src/ilPSP/ExtBinding/ilPSP.ExternalBinding/ExternalBinding.cs:15-75 (int ierr)
+ *
+ * Threading: a handle is not thread-safe; use one handle per host thread.  Each solver handle owns one CUDA
+ * stream; host-pointer calls are synchronous with respect to the caller.
+ */
+#ifndef BSGPU_H
+#define BSGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define BSGPU_API __declspec(dllexport)
+#else
+#define BSGPU_API __attribute__((visibility("default")))
+#endif
+
+/* ---- status codes (ISmootherTemplate / LAPACK-info conventions mapped to ints) --------------------------- */
+enum {
+  BSGPU_OK = 0,
+  BSGPU_ERR_ARGUMENT = 1,      /* ArgumentException: length / partition mismatch, bad handle, bad config   */
+  BSGPU_ERR_CUDA = 2,          /* CUDA runtime error (see bsgpu_last_error)                                */
+  BSGPU_ERR_ARITHMETIC = 3,    /* ArithmeticException: NaN/Inf, zero pivot, residual increase, breakdown    */
+  BSGPU_ERR_NOMEM = 4,         /* device allocation failed                                                 */
+  BSGPU_ERR_UNSUPPORTED = 5,   /* feature/size not supported by this build                                 */
+  BSGPU_ERR_TIMEOUT = 6        /* a bounded device-side wait gave up                                       */
+};
+
+/* pointer-kind flag for creation functions */
+enum { BSGPU_HOST_POINTERS = 0, BSGPU_DEVICE_POINTERS = 1 };
+
+typedef struct bsgpu_matrix_s* bsgpu_matrix_t;
+typedef struct bsgpu_mgop_s* bsgpu_mgop_t;
+typedef struct bsgpu_solver_s* bsgpu_solver_t;
+
+/* ---- library ------------------------------------------------------------------------------------------- */
+BSGPU_API int bsgpu_get_version(int* major, int* minor);
+/* Copies the message of the last failed call on this host thread into buf (NUL-terminated). */
+BSGPU_API int bsgpu_last_error(char* buf, size_t len);
+/* Number of kernels this library has launched in this process (tracing; FuncTrace/BlockTrace counterpart,
+ * src/ilPSP/layer_1.2-ilPSP/ilPSP/Tracing.cs:703,806). */
+BSGPU_API int bsgpu_get_launch_count(uint64_t* n);
+/* Selects the CUDA device used by handles created afterwards on this host thread. */
+BSGPU_API int bsgpu_set_device(int device);
+
+/* ---- BlockMsrMatrix (BlockMsrMatrix.cs:191) ------------------------------------------------------------ *
+ * nb block rows/columns; block i has nspc[i]*Np rows (nspc == NULL: one species); row_ptr[nb+1] and
+ * col_idx[nnzb] are the block-CSR structure with block columns ascending inside a block row (the
+ * SortedDictionary order of BlockMsrMatrix.cs:315); values holds the blocks row-major and concatenated in that
+ * order (the layout ReadBlock, BlockMsrMatrix.cs:1743, returns).  The library re-packs them into its own
+ * device layout.  flags: BSGPU_HOST_POINTERS or BSGPU_DEVICE_POINTERS for all four arrays. */
+BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, const int32_t* nspc,
+                                  const int64_t* row_ptr, const int32_t* col_idx, const double* values,
+                                  int32_t flags);
+BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A);
+BSGPU_API int bsgpu_matrix_get_info(bsgpu_matrix_t A, int64_t* nrows, int64_t* nb, int64_t* nnzb, int32_t* Np);
+/* Copies the values back in the creation layout (row-major blocks) to a host or device buffer. */
+BSGPU_API int bsgpu_matrix_read_values(bsgpu_matrix_t A, double* values, int32_t flags);
+/* BlockMsrMatrix.SpMV (BlockMsrMatrix.cs:2970): y = alpha*A*x + beta*y on host vectors of length nrows.
+ * x and y must not alias (ArgumentException in the reference).  beta == 0: y is not read. */
+BSGPU_API int bsgpu_matrix_spmv(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y);
+/* Same on device vectors, asynchronous on `stream` (NULL = the legacy default stream). */
+BSGPU_API int bsgpu_matrix_spmv_device(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y,
+                                       void* stream);
+/* FP32 copy of the values (for the single-precision preconditioner path) and its SpMV on float vectors. */
+BSGPU_API int bsgpu_matrix_create_single(bsgpu_matrix_t A, bsgpu_matrix_t* A32);
+BSGPU_API int bsgpu_matrix_spmv_device_f32(bsgpu_matrix_t A32, float alpha, const float* x, float beta, float* y,
+                                           void* stream);
+/* Sub-matrix of the leading `keep` modes of every species in every block (GridAndDegRestriction.cs:47-99). */
+BSGPU_API int bsgpu_matrix_restrict(bsgpu_matrix_t A, int32_t keep, bsgpu_matrix_t* Asub);
+
+/* ---- MultigridOperator change of basis (MultigridOperator.cs:650-700) ---------------------------------- *
+ * mode 0 = Eye, 1 = DiagBlockEquilib (SymmInv per diagonal block, MultigridOperator_ChangeOfBasis.cs:624).
+ * The operator seen by the solvers is L*A*L^T; B~ = L*B, X = L^T*X~. */
+enum { BSGPU_COB_EYE = 0, BSGPU_COB_DIAG_BLOCK_EQUILIB = 1 };
+BSGPU_API int bsgpu_mgop_create(bsgpu_mgop_t* op, bsgpu_matrix_t A, int32_t mode);
+BSGPU_API int bsgpu_mgop_destroy(bsgpu_mgop_t op);
+/* Borrowed handle of the transformed operator (owned by op). */
+BSGPU_API int bsgpu_mgop_get_operator(bsgpu_mgop_t op, bsgpu_matrix_t* Aop);
+/* Per-block L factors, row-major, concatenated in block order (host buffer). */
+BSGPU_API int bsgpu_mgop_read_left_cob(bsgpu_mgop_t op, double* L);
+
+/* ---- solvers (ISolverSmootherTemplate / ISolverFactory) ------------------------------------------------ */
+enum {
+  BSGPU_SOLVER_SOFTPCG = 0,     /* SoftPCG.cs:113 with a block-Jacobi preconditioner (or none)              */
+  BSGPU_SOLVER_FGMRES_PMG = 1,  /* FlexGMRES.cs:144 (Saad FGMRES(m)) preconditioned by one p-MG V-cycle     */
+  BSGPU_SOLVER_ORTHOMG = 2,     /* PmgConfig.cs:80 OrthonormalizationMultigrid p-multigrid as the solver    */
+  BSGPU_SOLVER_BLOCKJACOBI = 3  /* BlockJacobi.cs:35 as a standalone smoother                               */
+};
+enum { BSGPU_TERM_DEFAULT = 0 /* R < R0*tol + tol */, BSGPU_TERM_RELATIVE = 1 /* R < R0*tol */ };
+enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1 };
+enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in FP32, outer FP64 */ };
+
+typedef struct {
+  int32_t solver;           /* BSGPU_SOLVER_*                                                   */
+  int32_t termination;      /* BSGPU_TERM_*                                                     */
+  double tol;               /* ConvergenceCriterion (IterativeSolverConfig.cs:40), default 1e-10 */
+  int32_t max_iter;         /* MaxSolverIterations, default 300                                 */
+  int32_t min_iter;         /* MinSolverIterations, default 1                                   */
+  int32_t max_krylov;       /* FGMRESConfig.MaxKrylovDim                                        */
+  int32_t n_levels;         /* p-levels including the coarsest                                  */
+  int32_t level_keep[8];    /* modes per species kept on each level (level_keep[0] = Np)        */
+  int32_t post_sweeps;      /* NoOfPostSmootherSweeps (PmgConfig: 10)                           */
+  int32_t bj_iters;         /* BlockJacobi.NoOfIterations (<0: no preconditioner for SoftPCG)   */
+  double bj_omega;          /* BlockJacobi.omega                                                */
+  int32_t coarse_kind;      /* BSGPU_COARSE_*                                                   */
+  double coarse_tol;        /* relative tolerance of the PCG coarse solve                       */
+  int32_t coarse_max_iter;
+  int32_t sub_max_iter;     /* intermediate-level OrthoMG iteration limit (PmgConfig: 100)      */
+  double sub_reduction;     /* intermediate-level residual reduction (PmgConfig: 0.1)           */
+  int32_t precision;        /* BSGPU_PRECISION_*                                                */
+  int32_t reserved[16];
+} bsgpu_solver_config;
+
+typedef struct {
+  int32_t iterations;       /* ThisLevelIterations                                              */
+  int32_t nested;           /* IterationsInNested                                               */
+  int32_t converged;        /* Converged                                                        */
+  int32_t n_history;        /* entries written to the history buffer                            */
+  double res0, res;         /* initial and final residual norms (transformed basis)             */
+  double seconds;           /* device time of the solve                                         */
+} bsgpu_solve_stats;
+
+BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg);
+BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgpu_solver_config* cfg);
+BSGPU_API int bsgpu_solver_destroy(bsgpu_solver_t s);
+/* ISolverSmootherTemplate.Solve via MultigridOperator.UseSolver: X (initial guess in, solution out) and B in the
+ * original basis, host vectors.  Non-convergence is not an error (stats->converged = 0). */
+BSGPU_API int bsgpu_solver_solve(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats);
+/* Same with device vectors; synchronous on return. */
+BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats);
+/* Residual-norm history of the last solve (outer iterations), up to cap entries. */
+BSGPU_API int bsgpu_solver_get_history(bsgpu_solver_t s, double* hist, int32_t cap, int32_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSGPU_H */

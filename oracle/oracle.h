@@ -1,0 +1,54 @@
+/* ORACLE -- test infrastructure only (CPU restatement of the BoSSS solver path; see oracle.cpp). */
+#ifndef BOSSS_ORACLE_H
+#define BOSSS_ORACLE_H
+#include <stdint.h>
+
+enum { OR_OK = 0, OR_ERR_ARGUMENT = 1, OR_ERR_ARITHMETIC = 3 };
+enum { OR_SOLVER_PCG = 0, OR_SOLVER_FGMRES_PMG = 1, OR_SOLVER_ORTHOMG = 2 };
+enum { OR_COARSE_DENSE = 0, OR_COARSE_PCG = 1 };
+
+/* Block-sparse matrix: block i has nspc[i]*Np rows (nspc NULL: 1 species); blocks row-major, concatenated in
+ * BSR order (block rows ascending, block columns ascending). */
+typedef struct {
+  int64_t nb;
+  int32_t Np;
+  const int32_t* nspc;
+  const int64_t* row_ptr;
+  const int32_t* col_idx;
+  const double* values;
+} or_bsr;
+
+typedef struct {
+  int32_t solver;
+  int32_t top_mode; /* 0: R < R0*tol + tol (IterativeSolverConfig.DefaultTermination), 1: R < R0*tol */
+  double tol;
+  int32_t max_iter, min_iter;
+  int32_t max_krylov;
+  int32_t n_levels;
+  int32_t level_keep[8]; /* modes per species kept on each level; level_keep[0] = Np */
+  int32_t post_sweeps, bj_iters;
+  double bj_omega;
+  int32_t coarse_kind;
+  double coarse_tol;
+  int32_t coarse_max_iter;
+  int32_t sub_max_iter;
+  double sub_reduction;
+  int32_t reference_fgmres_defect;
+} or_solver_cfg;
+
+typedef struct {
+  int32_t iterations, nested, converged, n_hist;
+  double res0, res;
+} or_stats;
+
+const char* or_last_error(void);
+int or_set_threads(int n);
+int or_spmv(const or_bsr* m, double alpha, const double* x, double beta, double* y);
+int or_symminv(int n, double* M, double* L);
+int or_invert(int n, double* A);
+int or_change_of_basis(const or_bsr* m, double* values_out, double* L_out);
+int or_restrict(const or_bsr* m, int keep, double* values_out, int64_t* map_out);
+int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const double* b);
+int or_solve(const or_bsr* m, const or_solver_cfg* c, const double* b, double* x, or_stats* stats, double* hist,
+             int hist_cap);
+#endif

@@ -1,0 +1,61 @@
+"""CPU tests of the C-ABI library: it loads, exports every symbol the header declares, and fails loudly."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from bosss_b200 import native as nat
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "bsgpu.h")).read()
+    return sorted(set(re.findall(r"BSGPU_API\s+int\s+(bsgpu_\w+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    assert header_symbols() == sorted(nat.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", nat.LIB_PATH], capture_output=True, text=True, check=True)
+    exported = set(re.findall(r"\sT\s(bsgpu_\w+)", out.stdout))
+    missing = [s for s in header_symbols() if s not in exported]
+    assert not missing, missing
+    lib = nat.lib()
+    for s in header_symbols():
+        assert getattr(lib, s) is not None
+
+
+def test_version_and_error_reporting():
+    import ctypes as C
+    a, b = C.c_int(), C.c_int()
+    assert nat.lib().bsgpu_get_version(C.byref(a), C.byref(b)) == 0
+    assert (a.value, b.value) >= (0, 1)
+    # a null handle is an argument error, reported through bsgpu_last_error
+    rc = nat.lib().bsgpu_matrix_get_info(None, None, None, None, None)
+    assert rc == nat.ERR_ARGUMENT
+    assert "null" in nat.last_error()
+
+
+def test_no_silent_fallback_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    from bosss_b200 import assembly as A
+    from bosss_b200.solvers import BlockMsrMatrix
+    s = A.poisson_3d(2, 1)
+    with pytest.raises(nat.BsgpuError):
+        BlockMsrMatrix.from_system(s)
+
+
+def test_solver_config_defaults_follow_reference():
+    import ctypes as C
+    c = nat.SolverConfig()
+    assert nat.lib().bsgpu_solver_config_default(C.byref(c)) == 0
+    # IterativeSolverConfig.cs:19-40, PmgConfig.cs:160, FGMRES MaxKrylovDim
+    assert c.tol == 1e-10 and c.max_iter == 300 and c.min_iter == 1
+    assert c.post_sweeps == 10 and c.bj_iters == 1 and c.bj_omega == 1.0
+    assert c.sub_max_iter == 100 and c.sub_reduction == 0.1

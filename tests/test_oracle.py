@@ -1,0 +1,162 @@
+"""CPU tests: the oracle (CPU restatement) pinned against the reference's own known-answer tests.
+
+The reference ships no golden vectors; its solver-path tests pin tolerances (see the citations per test).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+from bosss_b200 import assembly as A
+from helpers import apply_blocks, l2_error, random_var_bsr, sip_cartesian1
+
+
+def test_testcartesian1_exactness():
+    """ipPoisson TestProgram.TestCartesian (Tests/TestProgram.cs:47-73): L2 error <= 5e-9 for a quadratic."""
+    g, s, exact = sip_cartesian1()
+    u = O.direct_solve(s)
+    assert l2_error(g, 2, u, exact) <= 5.0e-9
+
+
+@pytest.mark.parametrize("D,p", [(2, 2), (3, 2)])
+def test_convergence_slope(D, p):
+    """TestOperatorConvergence2D/3D (Tests/TestProgram.cs:321-406): slope >= p + 0.5."""
+    errs, hs = [], []
+    for n in ((4, 8) if D == 3 else (4, 8, 16)):
+        g = A.uniform_grid(D, n)
+        ex = lambda X: np.prod([np.sin(math.pi * x) for x in X], axis=0)
+        f = lambda X: D * math.pi ** 2 * ex(X)
+        s = A.assemble_sip(g, p, penalty=(p + 1) * (p + 2), rhs_f=f, quad=p + 4)
+        errs.append(l2_error(g, p, O.direct_solve(s), ex))
+        hs.append(1.0 / n)
+    slope = np.polyfit(np.log(hs), np.log(errs), 1)[0]
+    assert slope >= p + 0.5
+
+
+def test_spmv_matches_csr():
+    """Matrix_MPItest AllUpTest.SpMVTest (AllUpTest.cs:475-590): |err| <= 1e-10 |B| for SpMV(1.6, X, 0.5, B)."""
+    for s in (A.poisson_3d(6, 3), A.poisson_2d_c1(n=8)):
+        B = O.Bsr.of(s)
+        rng = np.random.default_rng(3)
+        X, Bv = rng.standard_normal(s.N), rng.standard_normal(s.N)
+        ref = 0.5 * Bv + 1.6 * (s.to_scipy() @ X)
+        out = O.spmv(B, 1.6, X, 0.5, Bv.copy())
+        assert np.linalg.norm(out - ref) <= 1e-10 * np.linalg.norm(ref)
+
+
+def test_spmv_uneven_blocks():
+    v = random_var_bsr(40, 10, seed=1)
+    B = O.Bsr.of(v)
+    x = np.random.default_rng(0).standard_normal(v.N)
+    ref = v.to_scipy() @ x
+    out = O.spmv(B, 1.0, x, 0.0, np.zeros(v.N))
+    assert np.linalg.norm(out - ref) <= 1e-13 * np.linalg.norm(ref)
+
+
+def test_symminv_equilibrates():
+    """SymmInv (MultigridOperator_ChangeOfBasis.cs:624): L M L^T = I for an SPD block, L lower triangular."""
+    rng = np.random.default_rng(0)
+    for n in (4, 10, 20):
+        Q = rng.standard_normal((n, n))
+        M = Q @ Q.T + n * np.eye(n)
+        L = O.symminv(M)
+        assert np.allclose(np.triu(L, 1), 0)
+        assert np.abs(L @ M @ L.T - np.eye(n)).max() < 1e-12
+
+
+def test_change_of_basis_and_restriction_consistency():
+    """The leading p-sub-block of L A L^T equals the transform of the restricted operator (lower-triangular L)."""
+    s = A.poisson_3d(4, 3)
+    B = O.Bsr.of(s)
+    vals, Lcat = O.change_of_basis(B)
+    rows = np.repeat(np.arange(s.nb), np.diff(s.row_ptr))
+    diag = vals.reshape(-1, 20, 20)[rows == s.col_idx]
+    assert np.abs(diag - np.eye(20)).max() < 1e-12
+    sub, _ = O.restrict(B, 10)
+
+    class S:  # restricted raw operator
+        Np, row_ptr, col_idx, values = 10, s.row_ptr, s.col_idx, sub
+    sub_t, _ = O.change_of_basis(O.Bsr.of(S))
+    lead = vals.reshape(-1, 20, 20)[:, :10, :10].reshape(-1)
+    assert np.abs(lead - sub_t).max() < 1e-10 * np.abs(lead).max()
+
+
+def test_restriction_is_polynomial_exact():
+    """MultigridTest (TestProgramLinearMG.cs:131-360): transfer of a degree-p' polynomial is exact (1e-10)."""
+    g = A.uniform_grid(3, 3)
+    f = lambda X: 1 + X[0] - 2 * X[1] * X[2] + X[2] ** 2
+    full = A.project_function(g, 3, f, q=6).reshape(-1)
+    low = A.project_function(g, 2, f, q=6).reshape(-1)
+    # the leading 10 of 20 modes hold the P2 projection
+    assert np.abs(full.reshape(-1, 20)[:, :10].reshape(-1) - low).max() < 1e-10
+    assert np.abs(full.reshape(-1, 20)[:, 10:]).max() < 1e-10
+
+
+def _transformed(s):
+    B = O.Bsr.of(s)
+    vals, Lcat = O.change_of_basis(B)
+
+    class T:
+        Np, row_ptr, col_idx, values = s.Np, s.row_ptr, s.col_idx, vals
+    Bt = O.Bsr.of(T)
+    bl = np.full(s.nb, s.Np)
+    return Bt, Lcat, bl
+
+
+def test_pcg_solves_c1_small():
+    """Block-Jacobi PCG (SoftPCG.cs:113-194) on the transformed 2-D operator reaches the direct solution."""
+    s = A.poisson_2d_c1(n=16)
+    Bt, Lcat, bl = _transformed(s)
+    bt = apply_blocks(Lcat, bl, s.rhs)
+    r = O.solve(Bt, bt, O.SolverConfig(solver=O.PCG, tol=1e-12, top_mode=O.TERM_RELATIVE, bj_iters=0))
+    x = apply_blocks(Lcat, bl, r.x, transpose=True)
+    xd = O.direct_solve(s)
+    assert r.converged
+    assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("kind", [O.FGMRES_PMG, O.ORTHOMG])
+def test_pmg_solvers_small(kind):
+    """FGMRES(30) with a 3-level p-MG V-cycle, and OrthoMG p-MG (PmgConfig.cs:80-245), 3-D p = 3."""
+    s = A.poisson_3d(6, 3)
+    Bt, Lcat, bl = _transformed(s)
+    bt = apply_blocks(Lcat, bl, s.rhs)
+    cfg = O.SolverConfig(solver=kind, tol=1e-11, top_mode=O.TERM_RELATIVE, level_keep=(20, 10, 4),
+                         coarse_kind=O.COARSE_PCG, coarse_tol=1e-4)
+    r = O.solve(Bt, bt, cfg)
+    x = apply_blocks(Lcat, bl, r.x, transpose=True)
+    xd = O.direct_solve(s)
+    assert r.converged and r.iterations < 40
+    assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+def test_reference_fgmres_defect_is_richardson():
+    """FlexGMRES.cs:259-260 discards the least-squares solution: with the flag the method needs far more
+    iterations than Saad's FGMRES on the same system."""
+    s = A.poisson_3d(4, 2)
+    Bt, Lcat, bl = _transformed(s)
+    bt = apply_blocks(Lcat, bl, s.rhs)
+    base = dict(solver=O.FGMRES_PMG, tol=1e-8, top_mode=O.TERM_RELATIVE, level_keep=(10, 4), max_iter=60,
+                coarse_kind=O.COARSE_PCG, coarse_tol=1e-2, max_krylov=10)
+    good = O.solve(Bt, bt, O.SolverConfig(**base))
+    bad = O.solve(Bt, bt, O.SolverConfig(**base, reference_fgmres_defect=True))
+    assert good.converged
+    assert bad.iterations > good.iterations
+
+
+def test_blockjacobi_two_updates():
+    """BlockJacobi with NoOfIterations = 1 performs two updates x <- x + D^-1 (b - A x) from x = 0."""
+    v = random_var_bsr(30, 4, seed=2, spd=True)
+    B = O.Bsr.of(v)
+    x = O.blockjacobi(B, np.zeros(v.N), v.rhs, iters=1)
+    M = v.to_scipy().toarray()
+    D = np.zeros_like(M)
+    i0 = np.concatenate([[0], np.cumsum(v.block_len)])
+    for i in range(v.nb):
+        sl = slice(i0[i], i0[i + 1])
+        D[sl, sl] = M[sl, sl]
+    Di = np.linalg.inv(D)
+    x1 = Di @ v.rhs
+    x2 = x1 + Di @ (v.rhs - M @ x1)
+    assert np.abs(x - x2).max() < 1e-12 * np.abs(x2).max()
