@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--p", type=int, default=3)
     ap.add_argument("--spmv-repeats", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spmv-only", action="store_true",
+                    help="only the stand-alone SpMV timing (profiling runs; prints a short JSON line)")
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
@@ -266,6 +268,10 @@ def run_ours(args):
     spmv32_ms = e0.elapsed_time(e1) / args.spmv_repeats
     nbytes32 = s.nnzb * s.Np * s.Np * 4 + s.nnzb * 4 + (s.nb + 1) * 8 + 2 * s.N * 4
     del A32, x32, y32
+    if args.spmv_only:
+        print(json.dumps({"spmv_fp64_gbs": spmv_gbs, "spmv_fp64_ms": spmv_avg, "bytes": nbytes,
+                          "spmv_fp32_gbs": nbytes32 / (spmv32_ms * 1e-3) / 1e9, "n": args.n, "p": args.p}))
+        return
 
     pmg = PmgConfig(DegreeHierarchy=levels_for(args.p), CoarseTolerance=1e-3)
     mk = lambda mixed: FGMRESConfig(ConvergenceCriterion=TOL, termination="relative", MaxKrylovDim=30,

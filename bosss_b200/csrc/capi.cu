@@ -340,6 +340,36 @@ BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const doubl
   });
 }
 
+BSGPU_API int bsgpu_solver_set_tracing(bsgpu_solver_t s, int32_t on) {
+  return guarded([&] {
+    require(s != nullptr, "null solver");
+    s->tree->ctx->tracing = on != 0;
+    for (auto& e : s->tree->ctx->trace) {
+      e.calls = 0;
+      e.seconds = 0;
+      e.iterations = 0;
+    }
+  });
+}
+
+BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len) {
+  return guarded([&] {
+    require(s != nullptr && buf != nullptr && len > 0, "null argument");
+    std::string out = "[";
+    char tmp[512];
+    bool first = true;
+    for (auto& e : s->tree->ctx->trace) {
+      std::snprintf(tmp, sizeof(tmp), "%s{\"name\": \"%s\", \"calls\": %ld, \"seconds\": %.6f, \"iterations\": %ld}",
+                    first ? "" : ", ", e.name.c_str(), e.calls, e.seconds, e.iterations);
+      out += tmp;
+      first = false;
+    }
+    out += "]";
+    std::strncpy(buf, out.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  });
+}
+
 BSGPU_API int bsgpu_solver_get_history(bsgpu_solver_t s, double* hist, int32_t cap, int32_t* n) {
   return guarded([&] {
     require(s != nullptr, "null solver");

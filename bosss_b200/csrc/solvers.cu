@@ -1,6 +1,8 @@
 // Solver tree of the hot path (see solvers.cuh).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "solvers.cuh"
@@ -44,6 +46,31 @@ void Ctx::check_flag(const int* f, const char* what) {
   if (h) {
     BSGPU_CUDA(cudaMemsetAsync(const_cast<int*>(f), 0, sizeof(int), st));
     throw Error(BSGPU_ERR_ARITHMETIC, what);
+  }
+}
+
+int Ctx::trace_id(const std::string& name) {
+  for (size_t i = 0; i < trace.size(); ++i)
+    if (trace[i].name == name) return (int)i;
+  trace.push_back(TraceEntry{name});
+  return (int)trace.size() - 1;
+}
+
+static double wall_now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+TraceScope::TraceScope(Ctx& ctx, int id_) : c(ctx), id(id_) {
+  if (c.tracing && id >= 0) {
+    cudaStreamSynchronize(c.st);
+    t0 = wall_now();
+  }
+}
+TraceScope::~TraceScope() {
+  if (c.tracing && id >= 0) {
+    cudaStreamSynchronize(c.st);
+    c.trace[id].seconds += wall_now() - t0;
+    c.trace[id].calls += 1;
   }
 }
 
@@ -101,6 +128,7 @@ struct BlockJacobiT : Solver<T> {
     tmp.alloc(std::max<int64_t>(A->N, 1));
   }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
     const int n = updates;
     const T* src = X;
     for (int s = 0; s < n; ++s) {
@@ -199,6 +227,7 @@ struct PCGT : Solver<T> {
       copy_vec(out, in, A->N, c.st);
   }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
     const int64_t N = A->N;
     cudaStream_t st = c.st;
     if (zero)
@@ -259,6 +288,7 @@ struct PCGT : Solver<T> {
       this->converged = st0.second;
     }
     this->this_level_iterations = it;
+    if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += it;
   }
 };
 
@@ -420,6 +450,7 @@ struct OrthoMGT : Solver<T> {
     return s;
   }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
     if (zero)
       copy_vec(Res0.p, B, N, c.st);
     else
@@ -472,6 +503,7 @@ struct OrthoMGT : Solver<T> {
       if (termPost) break;
       this->this_level_iterations++;
       this->history.push_back(rn);
+      if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += 1;
     }
   }
 };
@@ -503,6 +535,7 @@ struct GridAndDegT : Solver<T> {
   }
   int nested() const override { return lower ? lower->this_level_iterations + lower->nested() : 0; }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
     restrict_gather(B, bLo.p, sub->N, A->Np, keep, map.p, c.st);
     const T* a[1] = {bLo.p};
     dots(c.red, 1, a, a, sub->N, d_norm, 1, c.st);
@@ -591,6 +624,7 @@ struct FlexGMRES : Solver<double> {
     axpys(j + 1, d_h + off, nullptr, -1.0, vx.data(), W, N, c.st);
   }
   void solve(Ctx& c, double* X, const double* B, bool zero) override {
+    TraceScope ts(c, this->trace);
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
     int iIter = 0;
     double r0 = 0;
@@ -610,6 +644,7 @@ struct FlexGMRES : Solver<double> {
       if (!st.first || st.second) {
         this->converged = st.second;
         this->this_level_iterations = iIter;
+        if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += iIter;
         return;
       }
       axpby(1.0 / r, R0.p, 0.0, V[0].p, N, c.st);
@@ -693,7 +728,9 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
     ct.tol = cfg.coarse_tol;
     ct.max_iter = cfg.coarse_max_iter;
     ct.min_iter = 0;
-    return std::make_unique<PCGT<T>>(c, A64, AT, true, ct);
+    auto pcg = std::make_unique<PCGT<T>>(c, A64, AT, true, ct);
+    pcg->trace = c.trace_id("L" + std::to_string(level) + ".CoarsePCG");
+    return pcg;
   }
   Term lt = top;
   if (level > 0) {
@@ -701,14 +738,18 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
     lt.reduction = cfg.sub_reduction;
     lt.max_iter = cfg.sub_max_iter;
   }
+  const std::string lv = "L" + std::to_string(level);
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
+  omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = cfg.post_sweeps;
   omg->post = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
+  omg->post->trace = c.trace_id(lv + ".BlockJacobi");
   const int keep = cfg.level_keep[level + 1];
   t.owned.emplace_back(matrix_restrict(*A64, keep, c.st));
   const Matrix* sub64 = t.owned.back().get();
   const Matrix* subT = level_matrix<T>(t, sub64);
   auto gr = std::make_unique<GridAndDegT<T>>(c, AT, subT, keep);
+  gr->trace = c.trace_id(lv + ".GridAndDegRestriction");
   gr->lower = build_level<T>(t, sub64, subT, level + 1, top);
   omg->coarse = std::move(gr);
   return omg;
@@ -721,6 +762,8 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg) {
   require(cfg.n_levels >= 1 && cfg.n_levels <= 8, "n_levels must be in 1..8");
   auto t = std::make_unique<Tree>();
   t->ctx = std::make_unique<Ctx>();
+  const char* tr = std::getenv("BSGPU_TRACE");
+  t->ctx->tracing = tr != nullptr && tr[0] != '\0' && tr[0] != '0';
   t->A = A;
   t->cfg = cfg;
   Term top;
@@ -738,6 +781,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg) {
     case BSGPU_SOLVER_SOFTPCG: {
       require(!mixed, "mixed precision is available for the FGMRES preconditioner", BSGPU_ERR_UNSUPPORTED);
       t->top = std::make_unique<PCGT<double>>(*t->ctx, A, A, cfg.bj_iters >= 0, top);
+      t->top->trace = t->ctx->trace_id("SoftPCG");
       break;
     }
     case BSGPU_SOLVER_BLOCKJACOBI:
@@ -753,6 +797,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg) {
       one.mode = 2;
       one.max_iter = 1;
       auto f = std::make_unique<FlexGMRES>(*t->ctx, A, cfg.max_krylov, top);
+      f->trace = t->ctx->trace_id("FlexGMRES");
       if (mixed) {
         auto ad = std::make_unique<MixedAdapter>(A->N);
         ad->inner = build_level<float>(*t, A, level_matrix<float>(*t, A), 0, one);

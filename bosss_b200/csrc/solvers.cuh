@@ -32,6 +32,28 @@ struct Ctx {
     return hscal[d - dscal.p];
   }
   void check_flag(const int* f, const char* what);
+
+  // Tracing (counterpart of ilPSP FuncTrace/BlockTrace, Tracing.cs:703,806): per named block, the number of
+  // calls, inclusive wall time (the stream is synchronised at block exit when tracing is on) and iterations.
+  struct TraceEntry {
+    std::string name;
+    long calls = 0;
+    double seconds = 0;
+    long iterations = 0;
+  };
+  bool tracing = false;
+  std::vector<TraceEntry> trace;
+  int trace_id(const std::string& name);
+};
+
+// Scoped trace block; no-op unless ctx.tracing.
+struct TraceScope {
+  Ctx& c;
+  int id;
+  double t0 = 0;
+  long* iters_out = nullptr;
+  TraceScope(Ctx& ctx, int id_);
+  ~TraceScope();
 };
 
 template <typename T>
@@ -43,6 +65,7 @@ struct Solver {
   int this_level_iterations = 0;
   bool converged = false;
   std::vector<double> history;
+  int trace = -1;  // trace entry of this solver
 };
 
 // Termination criteria (IterativeSolverConfig.cs:48-62, PmgConfig.cs:202-215).

@@ -26,7 +26,7 @@ EXPORTS = [
     "bsgpu_matrix_restrict",
     "bsgpu_mgop_create", "bsgpu_mgop_destroy", "bsgpu_mgop_get_operator", "bsgpu_mgop_read_left_cob",
     "bsgpu_solver_config_default", "bsgpu_solver_create", "bsgpu_solver_destroy", "bsgpu_solver_solve",
-    "bsgpu_solver_solve_device", "bsgpu_solver_get_history",
+    "bsgpu_solver_solve_device", "bsgpu_solver_get_history", "bsgpu_solver_set_tracing", "bsgpu_solver_get_trace",
 ]
 
 
@@ -92,6 +92,8 @@ def lib() -> C.CDLL:
             "bsgpu_solver_solve": [vp, vp, vp, vp],
             "bsgpu_solver_solve_device": [vp, vp, vp, vp],
             "bsgpu_solver_get_history": [vp, vp, i32, vp],
+            "bsgpu_solver_set_tracing": [vp, i32],
+            "bsgpu_solver_get_trace": [vp, C.c_char_p, C.c_size_t],
         }
         for name, args in sig.items():
             f = getattr(L, name)

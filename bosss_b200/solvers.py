@@ -330,6 +330,16 @@ class GpuSolver:
         nat.check(nat.lib().bsgpu_solver_get_history(self._h, nat.ptr(out), n.value, C.byref(n)))
         return out[:n.value]
 
+    def SetTracing(self, on: bool = True):
+        nat.check(nat.lib().bsgpu_solver_set_tracing(self._h, 1 if on else 0))
+
+    def Trace(self):
+        """Per-solver-block calls / inclusive seconds / iterations recorded while tracing was on."""
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        nat.check(nat.lib().bsgpu_solver_get_trace(self._h, buf, len(buf)))
+        return json.loads(buf.value.decode())
+
     def Dispose(self):
         if self._h is not None:
             nat.lib().bsgpu_solver_destroy(self._h)

@@ -149,6 +149,11 @@ BSGPU_API int bsgpu_solver_solve(bsgpu_solver_t s, double* X, const double* B, b
 BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats);
 /* Residual-norm history of the last solve (outer iterations), up to cap entries. */
 BSGPU_API int bsgpu_solver_get_history(bsgpu_solver_t s, double* hist, int32_t cap, int32_t* n);
+/* Per-block tracing (FuncTrace counterpart, Tracing.cs:703): when on, every solver of the tree records calls,
+ * inclusive seconds and iterations (the stream is synchronised at block boundaries, so leave it off when timing
+ * the whole solve).  Also switched on by the environment variable BSGPU_TRACE=1.  get_trace writes a JSON array. */
+BSGPU_API int bsgpu_solver_set_tracing(bsgpu_solver_t s, int32_t on);
+BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len);
 
 #ifdef __cplusplus
 }
