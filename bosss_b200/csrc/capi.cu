@@ -289,6 +289,10 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->sub_max_iter = 100;
     cfg->sub_reduction = 0.1;
     cfg->precision = BSGPU_PRECISION_FP64;
+    cfg->h_levels = 0;
+    cfg->h_sweeps = 3;
+    cfg->h_cycle = 1;
+    cfg->dense_limit = 1024;
   });
 }
 

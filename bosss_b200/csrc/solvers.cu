@@ -553,6 +553,57 @@ struct GridAndDegT : Solver<T> {
   }
 };
 
+// h-coarse correction: restrict by aggregate sums, solve the Galerkin operator, prolongate by injection.
+template <typename T>
+struct AggregationT : Solver<T> {
+  const Aggregation* g;
+  std::unique_ptr<Solver<T>> lower;
+  DBuf<T> xc, bc;
+  double* d_norm;
+  AggregationT(Ctx& c, const Aggregation* g_) : g(g_) {
+    xc.alloc(std::max<int64_t>(g->nc, 1));
+    bc.alloc(std::max<int64_t>(g->nc, 1));
+    d_norm = c.scal(1);
+  }
+  int nested() const override { return lower ? lower->this_level_iterations + lower->nested() : 0; }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    (void)zero;
+    agg_restrict(*g, B, bc.p, c.st);
+    const T* a[1] = {bc.p};
+    dots(c.red, 1, a, a, g->nc, d_norm, 1, c.st);
+    if (!(c.get(d_norm) > 0)) {
+      this->converged = true;
+      return;
+    }
+    fill(T(0), xc.p, g->nc, c.st);
+    lower->solve(c, xc.p, bc.p, true);
+    this->converged = lower->converged;
+    agg_prolong_add(*g, xc.p, X, c.st);
+  }
+};
+
+// Direct solve of the coarsest level by a dense inverse computed once in FP64 (DirectSolver, DirectSolver.cs:43).
+template <typename T>
+struct DenseDirectT : Solver<T> {
+  int n;
+  DBuf<T> inv;
+  DenseDirectT(Ctx& c, const Matrix* A64) : n((int)A64->N) {
+    std::vector<double> h;
+    dense_inverse(*A64, h, c.st);
+    inv.alloc(std::max<size_t>(h.size(), 1));
+    std::vector<T> ht(h.begin(), h.end());
+    if (!ht.empty()) BSGPU_CUDA(cudaMemcpy(inv.p, ht.data(), ht.size() * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    (void)zero;
+    dense_gemv(inv.p, B, X, n, c.st);
+    this->converged = true;
+    this->this_level_iterations = 1;
+  }
+};
+
 // FP64 interface around an FP32 solver (mixed-precision preconditioner).
 struct MixedAdapter : Solver<double> {
   std::unique_ptr<Solver<float>> inner;
@@ -715,6 +766,47 @@ const Matrix* level_matrix(Tree& t, const Matrix* A64) {
   }
 }
 
+// Aggregation levels below the last (p = 0) p-level: OrthoMG with h_cycle iterations per call, h_sweeps
+// block-Jacobi post-smoother sweeps and an aggregation coarse correction; the last level is solved densely.
+template <typename T>
+std::unique_ptr<Solver<T>> build_hlevel(Tree& t, const Matrix* A64, const Matrix* AT, int hl) {
+  const bsgpu_solver_config& cfg = t.cfg;
+  Ctx& c = *t.ctx;
+  const std::string lv = "H" + std::to_string(hl);
+  if (A64->N <= cfg.dense_limit) {
+    auto d = std::make_unique<DenseDirectT<T>>(c, A64);
+    d->trace = c.trace_id(lv + ".DenseDirect");
+    return d;
+  }
+  if (hl >= cfg.h_levels) {
+    Term ct;
+    ct.mode = 1;
+    ct.tol = cfg.coarse_tol;
+    ct.max_iter = cfg.coarse_max_iter;
+    ct.min_iter = 0;
+    auto pcg = std::make_unique<PCGT<T>>(c, A64, AT, true, ct);
+    pcg->trace = c.trace_id(lv + ".CoarsePCG");
+    return pcg;
+  }
+  Term ht;
+  ht.mode = 2;
+  ht.max_iter = std::max(1, cfg.h_cycle);
+  auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
+  omg->trace = c.trace_id(lv + ".OrthoMG");
+  omg->sweeps = cfg.h_sweeps;
+  omg->post = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
+  omg->post->trace = c.trace_id(lv + ".BlockJacobi");
+  t.aggs.emplace_back(matrix_aggregate(*A64, c.st));
+  const Aggregation* g = t.aggs.back().get();
+  const Matrix* c64 = g->coarse.get();
+  const Matrix* cT = level_matrix<T>(t, c64);
+  auto ag = std::make_unique<AggregationT<T>>(c, g);
+  ag->trace = c.trace_id(lv + ".Aggregation");
+  ag->lower = build_hlevel<T>(t, c64, cT, hl + 1);
+  omg->coarse = std::move(ag);
+  return omg;
+}
+
 // A64: FP64 level operator (factorisations are computed from it); AT: the same operator in the precision T the
 // level runs in (AT == A64 for T = double).
 template <typename T>
@@ -722,7 +814,15 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   const bsgpu_solver_config& cfg = t.cfg;
   Ctx& c = *t.ctx;
   if (level == cfg.n_levels - 1) {
-    require(cfg.coarse_kind == BSGPU_COARSE_PCG, "only the PCG coarse solve is available", BSGPU_ERR_UNSUPPORTED);
+    if (cfg.h_levels > 0 && A64->uniform && A64->Np == 1) return build_hlevel<T>(t, A64, AT, 0);
+    if (cfg.coarse_kind == BSGPU_COARSE_DENSE) {
+      require(A64->uniform && A64->Np == 1, "the dense coarse solve needs a p = 0 last level", BSGPU_ERR_UNSUPPORTED);
+      require(A64->N <= 4096, "the dense coarse solve is limited to 4096 unknowns", BSGPU_ERR_UNSUPPORTED);
+      auto d = std::make_unique<DenseDirectT<T>>(c, A64);
+      d->trace = c.trace_id("L" + std::to_string(level) + ".DenseDirect");
+      return d;
+    }
+    require(cfg.coarse_kind == BSGPU_COARSE_PCG, "unknown coarse solver", BSGPU_ERR_UNSUPPORTED);
     Term ct;
     ct.mode = 1;
     ct.tol = cfg.coarse_tol;

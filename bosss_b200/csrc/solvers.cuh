@@ -5,6 +5,7 @@
 #pragma once
 #include <memory>
 
+#include "aggregation.cuh"
 #include "blas1.cuh"
 #include "blockops.cuh"
 #include "matrix.cuh"
@@ -86,6 +87,7 @@ struct TreeConfig {
 struct Tree {
   std::unique_ptr<Ctx> ctx;
   std::vector<std::unique_ptr<Matrix>> owned;
+  std::vector<std::unique_ptr<Aggregation>> aggs;
   std::unique_ptr<Solver<double>> top;
   const Matrix* A = nullptr;
   bsgpu_solver_config cfg{};

@@ -36,7 +36,8 @@ class SolverConfig(C.Structure):
                 ("level_keep", C.c_int32 * 8), ("post_sweeps", C.c_int32), ("bj_iters", C.c_int32),
                 ("bj_omega", C.c_double), ("coarse_kind", C.c_int32), ("coarse_tol", C.c_double),
                 ("coarse_max_iter", C.c_int32), ("sub_max_iter", C.c_int32), ("sub_reduction", C.c_double),
-                ("precision", C.c_int32), ("reserved", C.c_int32 * 16)]
+                ("precision", C.c_int32), ("h_levels", C.c_int32), ("h_sweeps", C.c_int32), ("h_cycle", C.c_int32),
+                ("dense_limit", C.c_int32), ("reserved", C.c_int32 * 12)]
 
 
 class SolveStats(C.Structure):

@@ -192,7 +192,10 @@ class PmgConfig(IterativeSolverConfig):
     """PmgConfig.CreateInstanceImpl__Kummer with UseILU = false (block-Jacobi post-smoother on every level).
 
     ``DegreeHierarchy``: modes per species kept on each level, finest first (e.g. (20, 10, 4) for p = 3 -> 2 -> 1
-    in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative).
+    in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative), or densely
+    (``CoarseSolver = "dense"``, p = 0 levels up to 4096 unknowns).  With ``HLevels > 0`` and a p = 0 last level
+    (DegreeHierarchy ending in 1), up to ``HLevels`` aggregation h-levels follow, each an OrthoMG with
+    ``HCycle`` iterations and ``HSweeps`` post-smoother sweeps, down to ``DenseLimit`` unknowns.
     """
     DegreeHierarchy: tuple = (20, 10, 4)
     NoOfPostSmootherSweeps: int = 10
@@ -200,8 +203,13 @@ class PmgConfig(IterativeSolverConfig):
     BlockJacobiOmega: float = 1.0
     CoarseTolerance: float = 1e-3
     CoarseMaxIterations: int = 2000
+    CoarseSolver: str = "pcg"
     SubLevelMaxIterations: int = 100
     SubLevelReduction: float = 0.1
+    HLevels: int = 0
+    HSweeps: int = 3
+    HCycle: int = 1
+    DenseLimit: int = 1024
     UseILU: bool = False
 
     def _fill(self, c):
@@ -213,11 +221,15 @@ class PmgConfig(IterativeSolverConfig):
         c.post_sweeps = self.NoOfPostSmootherSweeps
         c.bj_iters = self.BlockJacobiIterations
         c.bj_omega = self.BlockJacobiOmega
-        c.coarse_kind = nat.COARSE_PCG
+        c.coarse_kind = nat.COARSE_DENSE if self.CoarseSolver == "dense" else nat.COARSE_PCG
         c.coarse_tol = self.CoarseTolerance
         c.coarse_max_iter = self.CoarseMaxIterations
         c.sub_max_iter = self.SubLevelMaxIterations
         c.sub_reduction = self.SubLevelReduction
+        c.h_levels = self.HLevels
+        c.h_sweeps = self.HSweeps
+        c.h_cycle = self.HCycle
+        c.dense_limit = self.DenseLimit
 
     def _config(self):
         c = self._base()

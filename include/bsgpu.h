@@ -127,7 +127,11 @@ typedef struct {
   int32_t sub_max_iter;     /* intermediate-level OrthoMG iteration limit (PmgConfig: 100)      */
   double sub_reduction;     /* intermediate-level residual reduction (PmgConfig: 0.1)           */
   int32_t precision;        /* BSGPU_PRECISION_*                                                */
-  int32_t reserved[16];
+  int32_t h_levels;         /* aggregation h-levels below a p = 0 last p-level (0: none)        */
+  int32_t h_sweeps;         /* post-smoother sweeps on the h-levels                             */
+  int32_t h_cycle;          /* OrthoMG iterations per call on the h-levels (1 = V-cycle)        */
+  int32_t dense_limit;      /* levels with at most this many unknowns are solved densely        */
+  int32_t reserved[12];
 } bsgpu_solver_config;
 
 typedef struct {

@@ -115,6 +115,33 @@ def test_fgmres_pmg_3d(cuda, mixed):
     assert abs(r.iterations - slv.ThisLevelIterations) <= (3 if not mixed else 5)
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_fgmres_pmg_with_h_levels(cuda, mixed):
+    """p-levels 3 -> 2 -> 1 -> 0, then aggregation h-levels on p = 0 down to a dense direct solve."""
+    s = A.poisson_3d(10, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4, 1), HLevels=4, HSweeps=3, DenseLimit=40)
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
+                       MixedPrecision=mixed).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged and slv.ThisLevelIterations < 40
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+def test_dense_coarse_solve(cuda):
+    s = A.poisson_3d(4, 2)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = PmgConfig(DegreeHierarchy=(10, 4, 1), CoarseSolver="dense")
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg]).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
 def test_orthomg_pmg_3d(cuda):
     s = A.poisson_3d(6, 2)
     op = MultigridOperator(BlockMsrMatrix.from_system(s))
