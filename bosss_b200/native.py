@@ -22,7 +22,8 @@ PRECISION_FP64, PRECISION_MIXED = 0, 1
 EXPORTS = [
     "bsgpu_get_version", "bsgpu_last_error", "bsgpu_get_launch_count", "bsgpu_set_device",
     "bsgpu_matrix_create", "bsgpu_matrix_destroy", "bsgpu_matrix_get_info", "bsgpu_matrix_read_values",
-    "bsgpu_matrix_spmv", "bsgpu_matrix_spmv_device", "bsgpu_matrix_create_single", "bsgpu_matrix_spmv_device_f32",
+    "bsgpu_matrix_spmv", "bsgpu_matrix_spmv_noalloc", "bsgpu_matrix_spmv_device", "bsgpu_matrix_create_single",
+    "bsgpu_matrix_spmv_device_f32",
     "bsgpu_matrix_restrict",
     "bsgpu_mgop_create", "bsgpu_mgop_destroy", "bsgpu_mgop_get_operator", "bsgpu_mgop_read_left_cob",
     "bsgpu_solver_config_default", "bsgpu_solver_create", "bsgpu_solver_destroy", "bsgpu_solver_solve",
@@ -79,6 +80,7 @@ def lib() -> C.CDLL:
             "bsgpu_matrix_get_info": [vp, vp, vp, vp, vp],
             "bsgpu_matrix_read_values": [vp, vp, i32],
             "bsgpu_matrix_spmv": [vp, dbl, vp, dbl, vp],
+            "bsgpu_matrix_spmv_noalloc": [vp, dbl, vp, dbl, vp],
             "bsgpu_matrix_spmv_device": [vp, dbl, vp, dbl, vp, vp],
             "bsgpu_matrix_create_single": [vp, vp],
             "bsgpu_matrix_spmv_device_f32": [vp, flt, vp, flt, vp, vp],

@@ -77,6 +77,14 @@ BSGPU_API int bsgpu_matrix_read_values(bsgpu_matrix_t A, double* values, int32_t
 /* BlockMsrMatrix.SpMV (BlockMsrMatrix.cs:2970): y = alpha*A*x + beta*y on host vectors of length nrows.
  * x and y must not alias (ArgumentException in the reference).  beta == 0: y is not read. */
 BSGPU_API int bsgpu_matrix_spmv(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y);
+/* Same as bsgpu_matrix_spmv but allocates no device memory, for callers that must not (a host program whose
+ * device memory is already committed to its own pool, or one that cannot afford the device-wide synchronisation
+ * cudaMalloc/cudaFree may cause).  No counterpart in the reference.  x and y are staged in a fixed array of
+ * 2 x 2^20 doubles that every GPU loading the library holds until exit, so nrows must be <= 1,048,576
+ * (BSGPU_ERR_ARGUMENT otherwise).  The first call on a device looks up that array's device address, so make it
+ * before any stream capture.  All calls share the array: calls that overlap on the GPU (several host threads)
+ * race. */
+BSGPU_API int bsgpu_matrix_spmv_noalloc(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y);
 /* Same on device vectors, asynchronous on `stream` (NULL = the legacy default stream). */
 BSGPU_API int bsgpu_matrix_spmv_device(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y,
                                        void* stream);
