@@ -505,6 +505,75 @@ def project_function(grid: RectilinearGrid, p: int, f: Callable, q: Optional[int
 
 
 # ----------------------------------------------------------------------------------------------------------------
+# h-levels: agglomeration of 2^D cells and exact polynomial prolongation
+# ----------------------------------------------------------------------------------------------------------------
+
+@dataclasses.dataclass
+class HProlongation:
+    """Prolongation from an agglomerated grid to the finer one, in the orthonormal DG basis of degree p.
+
+    Block-sparse: row block = fine cell, column block = coarse cell (its agglomerate), each block Np x Np
+    row-major; the counterpart of the prolongation operators of BoSSS's multigrid hierarchy on aggregation
+    grids (MultigridOperator.cs:774,815 Restrict/Prolongate; AggregationGridBasis.cs)."""
+    Np: int
+    nb_fine: int
+    nb_coarse: int
+    row_ptr: np.ndarray
+    col_idx: np.ndarray
+    values: np.ndarray   # [nb_fine, Np, Np]
+    coarse_grid: RectilinearGrid
+
+
+def _child_projection_1d(p: int, side: int) -> np.ndarray:
+    """T[j, k] = int_child psi^f_j psi^c_k with both bases orthonormal on their own interval (child = left/right half)."""
+    tg, wg = gauss(p + 2)
+    # fine reference coordinate t in [-1,1] -> coarse coordinate s = (t - 1)/2 (left) or (t + 1)/2 (right)
+    s = 0.5 * (tg + (1.0 if side else -1.0))
+    F = np.stack([psi(j, tg) for j in range(p + 1)])          # fine basis on its reference interval
+    Cc = np.stack([psi(k, s) for k in range(p + 1)])          # coarse basis evaluated in the child
+    # physical scaling: fine basis sqrt(2/h), coarse sqrt(2/(2h)); dx = h/2 dt  -> factor sqrt(1/2)
+    return (F * wg) @ Cc.T * math.sqrt(0.5)
+
+
+def h_prolongation(grid: RectilinearGrid, p: int) -> HProlongation:
+    """2^D -> 1 agglomeration of a uniformly refined grid (every direction even)."""
+    D = grid.D
+    assert all(n % 2 == 0 for n in grid.shape), "every direction needs an even number of cells"
+    modes = dg_modes(D, p)
+    Np = len(modes)
+    T = [_child_projection_1d(p, s) for s in (0, 1)]
+    cg = RectilinearGrid([np.asarray(grid.nodes[d])[::2] for d in range(D)])
+    mi = grid.cell_multi_index()
+    coarse = np.zeros(grid.ncells, dtype=np.int64)
+    child = np.zeros(grid.ncells, dtype=np.int64)
+    stride = 1
+    for d in range(D):
+        coarse += (mi[d] // 2) * stride
+        child += (mi[d] % 2) << d
+        stride *= cg.shape[d]
+    blocks = np.empty((2 ** D, Np, Np))
+    for c in range(2 ** D):
+        M = np.ones((Np, Np))
+        for d in range(D):
+            M = M * T[(c >> d) & 1][modes[:, d][:, None], modes[:, d][None, :]]
+        blocks[c] = M
+    return HProlongation(Np=Np, nb_fine=grid.ncells, nb_coarse=cg.ncells,
+                         row_ptr=np.arange(grid.ncells + 1, dtype=np.int64), col_idx=coarse.astype(np.int32),
+                         values=blocks[child], coarse_grid=cg)
+
+
+def h_hierarchy(grid: RectilinearGrid, p: int, min_cells: int = 64) -> list:
+    """Successive 2^D agglomerations while every direction stays even and the grid has more than min_cells."""
+    out = []
+    g = grid
+    while all(n % 2 == 0 for n in g.shape) and g.ncells > min_cells:
+        P = h_prolongation(g, p)
+        out.append(P)
+        g = P.coarse_grid
+    return out
+
+
+# ----------------------------------------------------------------------------------------------------------------
 # Seeded synthetic right-hand sides and coefficients
 # ----------------------------------------------------------------------------------------------------------------
 

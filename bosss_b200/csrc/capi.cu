@@ -17,6 +17,7 @@ struct bsgpu_mgop_s {
   bsgpu::DBuf<double> L;       // per-block left change of basis, row-major
   int mode = 0;
   bsgpu_matrix_s op_handle;    // borrowed handle returned by bsgpu_mgop_get_operator
+  std::vector<bsgpu::HostBsr> hprol;  // h-level prolongations below the coarsest p-level
   const bsgpu::Matrix* op() const { return mode == BSGPU_COB_EYE ? A : Aop.get(); }
 };
 
@@ -261,6 +262,28 @@ BSGPU_API int bsgpu_mgop_get_operator(bsgpu_mgop_t op, bsgpu_matrix_t* Aop) {
   });
 }
 
+BSGPU_API int bsgpu_mgop_add_h_level(bsgpu_mgop_t op, int32_t Np, int64_t nb_fine, int64_t nb_coarse,
+                                     const int64_t* row_ptr, const int32_t* col_idx, const double* values) {
+  return guarded([&] {
+    require(op && row_ptr && (col_idx || nb_fine == 0) && (values || nb_fine == 0), "null argument");
+    require(Np > 0 && nb_fine > 0 && nb_coarse > 0 && nb_coarse <= nb_fine, "bad h-level sizes");
+    if (!op->hprol.empty())
+      require(op->hprol.back().nb_cols == nb_fine, "h-level rows must equal the previous level's coarse blocks");
+    HostBsr P;
+    P.Np = Np;
+    P.nb_rows = nb_fine;
+    P.nb_cols = nb_coarse;
+    P.rp.assign(row_ptr, row_ptr + nb_fine + 1);
+    require(P.rp[0] == 0, "row_ptr[0] must be 0");
+    for (int64_t i = 0; i < nb_fine; ++i) require(P.rp[i + 1] >= P.rp[i], "row_ptr must be non-decreasing");
+    const int64_t nnzb = P.rp[nb_fine];
+    P.ci.assign(col_idx, col_idx + nnzb);
+    for (int32_t c : P.ci) require(c >= 0 && c < nb_coarse, "col_idx out of range");
+    P.v.assign(values, values + nnzb * (int64_t)Np * Np);
+    op->hprol.push_back(std::move(P));
+  });
+}
+
 BSGPU_API int bsgpu_mgop_read_left_cob(bsgpu_mgop_t op, double* L) {
   return guarded([&] {
     require(op && L, "null argument");
@@ -302,7 +325,11 @@ BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgp
     require(s && op && cfg, "null argument");
     auto h = std::make_unique<bsgpu_solver_s>();
     h->op = op;
-    h->tree.reset(build_tree(op->op(), *cfg));
+    OperatorInfo info;
+    info.top = op->A;
+    info.L = op->mode == BSGPU_COB_DIAG_BLOCK_EQUILIB ? op->L.p : nullptr;
+    info.hprol = &op->hprol;
+    h->tree.reset(build_tree(op->op(), *cfg, info));
     const int64_t N = std::max<int64_t>(op->A->N, 1);
     h->X.alloc(N); h->B.alloc(N); h->Xt.alloc(N); h->Bt.alloc(N);
     BSGPU_CUDA(cudaEventCreate(&h->e0));

@@ -591,6 +591,10 @@ struct DenseDirectT : Solver<T> {
   DenseDirectT(Ctx& c, const Matrix* A64) : n((int)A64->N) {
     std::vector<double> h;
     dense_inverse(*A64, h, c.st);
+    upload(h);
+  }
+  DenseDirectT(const std::vector<double>& h, int64_t n_) : n((int)n_) { upload(h); }
+  void upload(const std::vector<double>& h) {
     inv.alloc(std::max<size_t>(h.size(), 1));
     std::vector<T> ht(h.begin(), h.end());
     if (!ht.empty()) BSGPU_CUDA(cudaMemcpy(inv.p, ht.data(), ht.size() * sizeof(T), cudaMemcpyHostToDevice));
@@ -601,6 +605,178 @@ struct DenseDirectT : Solver<T> {
     dense_gemv(inv.p, B, X, n, c.st);
     this->converged = true;
     this->this_level_iterations = 1;
+  }
+};
+
+// Coarse correction through explicit restriction / prolongation matrices (MultigridOperator.Restrict /
+// Prolongate, MultigridOperator.cs:774,815): b_c = R b, solve on the coarser h-level, X += P x_c.
+template <typename T>
+struct TransferT : Solver<T> {
+  const Csr* P;
+  const Csr* R;
+  std::unique_ptr<Solver<T>> lower;
+  DBuf<T> xc, bc;
+  double* d_norm;
+  TransferT(Ctx& c, const Csr* P_, const Csr* R_) : P(P_), R(R_) {
+    xc.alloc(std::max<int64_t>(P->cols, 1));
+    bc.alloc(std::max<int64_t>(P->cols, 1));
+    d_norm = c.scal(1);
+  }
+  int nested() const override { return lower ? lower->this_level_iterations + lower->nested() : 0; }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    (void)zero;
+    csr_spmv(*R, T(1), B, T(0), bc.p, c.st);
+    const T* a[1] = {bc.p};
+    dots(c.red, 1, a, a, R->rows, d_norm, 1, c.st);
+    if (!(c.get(d_norm) > 0)) {
+      this->converged = true;
+      return;
+    }
+    fill(T(0), xc.p, P->cols, c.st);
+    lower->solve(c, xc.p, bc.p, true);
+    this->converged = lower->converged;
+    csr_spmv(*P, T(1), xc.p, T(1), X, c.st);
+  }
+};
+
+// Coarsest p-level: CG preconditioned by one smoothed-aggregation V-cycle (amg.cu) per iteration, to a relative
+// tolerance.  Stand-in for the reference's direct solve of this level (PmgConfig.cs:167-177).
+template <typename T>
+struct AmgPcgT : Solver<T> {
+  const AmgHierarchy* H;
+  std::vector<const Matrix*> Al;  // level operators in precision T
+  std::vector<DBuf<T>> lx, lb, lr;
+  DBuf<T> dense, r, z, p, q;
+  int nu;
+  Term term;
+  double* d_s;  // [0] rr, [1] rz, [2] pq
+  AmgPcgT(Tree& t, const AmgHierarchy* H_, const Matrix* AT, int sweeps, Term tm) : H(H_), nu(sweeps), term(tm) {
+    Ctx& c = *t.ctx;
+    const size_t nl = H->levels.size();
+    for (size_t l = 0; l < nl; ++l) {
+      const Matrix* A64 = H->levels[l].Aref;
+      if (l == 0)
+        Al.push_back(AT);
+      else if (sizeof(T) == 8)
+        Al.push_back(A64);
+      else {
+        t.owned.emplace_back(matrix_to_single(*A64, c.st));
+        Al.push_back(t.owned.back().get());
+      }
+      const int64_t n = std::max<int64_t>(H->levels[l].n, 1);
+      lx.emplace_back(n);
+      lb.emplace_back(n);
+      lr.emplace_back(n);
+    }
+    if (H->n_dense) {
+      dense.alloc(H->dense_inv.size());
+      std::vector<T> h(H->dense_inv.begin(), H->dense_inv.end());
+      BSGPU_CUDA(cudaMemcpy(dense.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    const int64_t N = std::max<int64_t>(H->levels[0].n, 1);
+    r.alloc(N); z.alloc(N); p.alloc(N); q.alloc(N);
+    d_s = c.scal(3);
+  }
+  const T* dinv(int l) const {
+    if constexpr (sizeof(T) == 8) return H->levels[l].dinv64.p;
+    else return H->levels[l].dinv32.p;
+  }
+  void smooth(Ctx& c, int l, T* X, const T* B, bool zero, int sweeps) {
+    const Matrix& A = *Al[l];
+    const T w = (T)H->levels[l].omega;
+    const int64_t n = H->levels[l].n;
+    for (int s = 0; s < sweeps; ++s) {
+      if (s == 0 && zero) {
+        jacobi_update(dinv(l), w, B, (const T*)nullptr, X, n, c.st);
+      } else {
+        spmv(A, T(1), X, T(0), (const T*)nullptr, lr[l].p, c.st);
+        jacobi_update(dinv(l), w, B, lr[l].p, X, n, c.st);
+      }
+    }
+  }
+  std::vector<int> tr_smooth, tr_transfer;
+  void trace_ids(Ctx& c) {
+    for (size_t l = 0; l < H->levels.size(); ++l) {
+      tr_smooth.push_back(c.trace_id("AMG" + std::to_string(l) + ".smooth(n=" + std::to_string(H->levels[l].n) + ")"));
+      tr_transfer.push_back(c.trace_id("AMG" + std::to_string(l) + ".transfer"));
+    }
+  }
+  void vcycle(Ctx& c, int l, T* X, const T* B, bool zero) {
+    const int last = (int)H->levels.size() - 1;
+    const AmgLevel& L = H->levels[l];
+    if (tr_smooth.empty()) trace_ids(c);
+    if (l == last) {
+      TraceScope ts(c, tr_smooth[l]);
+      if (H->n_dense)
+        dense_gemv(dense.p, B, X, (int)H->n_dense, c.st);
+      else
+        smooth(c, l, X, B, zero, 2 * nu);
+      return;
+    }
+    {
+      TraceScope ts(c, tr_smooth[l]);
+      smooth(c, l, X, B, zero, nu);
+    }
+    {
+      TraceScope ts(c, tr_transfer[l]);
+      spmv(*Al[l], T(-1), X, T(1), B, lr[l].p, c.st);
+      csr_spmv(*L.R, T(1), lr[l].p, T(0), lb[l + 1].p, c.st);
+    }
+    vcycle(c, l + 1, lx[l + 1].p, lb[l + 1].p, true);
+    {
+      TraceScope ts(c, tr_transfer[l]);
+      csr_spmv(*L.P, T(1), lx[l + 1].p, T(1), X, c.st);
+    }
+    TraceScope ts(c, tr_smooth[l]);
+    smooth(c, l, X, B, false, nu);
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    const Matrix& A = *Al[0];
+    const int64_t N = A.N;
+    if (zero)
+      copy_vec(r.p, B, N, c.st);
+    else
+      spmv(A, T(-1), X, T(1), B, r.p, c.st);
+    const T* rv[1] = {r.p};
+    dots(c.red, 1, rv, rv, N, d_s, 0, c.st);
+    const double rr0 = c.get(d_s);
+    if (!std::isfinite(rr0)) throw Error(BSGPU_ERR_ARITHMETIC, "AMG-PCG: NaN/Inf in the right-hand side");
+    this->history.assign(1, std::sqrt(rr0));
+    int it = 0;
+    if (rr0 > 0) {
+      vcycle(c, 0, z.p, r.p, true);
+      copy_vec(p.p, z.p, N, c.st);
+      const T* zv[1] = {z.p};
+      dots(c.red, 1, rv, zv, N, d_s + 1, 0, c.st);
+      double rz = c.get(d_s + 1);
+      const T* pv[1] = {p.p};
+      const T* qv[1] = {q.p};
+      for (it = 1; it <= term.max_iter; ++it) {
+        spmv(A, T(1), p.p, T(0), (const T*)nullptr, q.p, c.st);
+        dots(c.red, 1, pv, qv, N, d_s + 2, 0, c.st);
+        const double pq = c.get(d_s + 2);
+        const double alpha = rz / pq;
+        if (!std::isfinite(alpha)) throw Error(BSGPU_ERR_ARITHMETIC, "AMG-PCG: breakdown");
+        const double ha[1] = {alpha}, hm[1] = {-alpha};
+        axpys(1, nullptr, ha, 1.0, pv, X, N, c.st);
+        axpys(1, nullptr, hm, 1.0, qv, r.p, N, c.st);
+        dots(c.red, 1, rv, rv, N, d_s, 0, c.st);
+        const double rr = c.get(d_s);
+        this->history.push_back(std::sqrt(rr));
+        if (rr <= term.tol * term.tol * rr0) break;
+        vcycle(c, 0, z.p, r.p, true);
+        dots(c.red, 1, rv, zv, N, d_s + 1, 0, c.st);
+        const double rz_new = c.get(d_s + 1);
+        axpby(T(1), z.p, T(rz_new / rz), p.p, N, c.st);
+        rz = rz_new;
+      }
+      if (it > term.max_iter) it = term.max_iter;
+    }
+    this->converged = this->history.back() <= term.tol * this->history.front() || rr0 == 0;
+    this->this_level_iterations = it;
+    if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += it;
   }
 };
 
@@ -807,6 +983,54 @@ std::unique_ptr<Solver<T>> build_hlevel(Tree& t, const Matrix* A64, const Matrix
   return omg;
 }
 
+// h-multigrid below the coarsest p-level: level k of the hierarchy is an OrthoMG with block-Jacobi smoothing and
+// a TransferT coarse correction; level 0 (the p-level itself) iterates to the coarse tolerance, the others run
+// h_cycle iterations; the last level is solved densely.
+template <typename T>
+std::unique_ptr<Solver<T>> build_hmg_level(Tree& t, const HmgHierarchy* H, const Matrix* AT, size_t k) {
+  const bsgpu_solver_config& cfg = t.cfg;
+  Ctx& c = *t.ctx;
+  const std::string lv = "HMG" + std::to_string(k);
+  const Matrix* A64 = H->levels[k].Aref;
+  if (k + 1 == H->levels.size()) {
+    if (H->n_dense) {
+      auto d = std::make_unique<DenseDirectT<T>>(H->dense_inv, H->n_dense);
+      d->trace = c.trace_id(lv + ".DenseDirect");
+      return d;
+    }
+    Term ct;
+    ct.mode = 1;
+    ct.tol = cfg.coarse_tol;
+    ct.max_iter = cfg.coarse_max_iter;
+    ct.min_iter = 0;
+    auto pcg = std::make_unique<PCGT<T>>(c, A64, AT, true, ct);
+    pcg->trace = c.trace_id(lv + ".CoarsePCG");
+    return pcg;
+  }
+  Term ht;
+  if (k == 0) {
+    ht.mode = 1;
+    ht.tol = cfg.coarse_tol;
+    ht.max_iter = cfg.coarse_max_iter;
+    ht.min_iter = 1;
+  } else {
+    ht.mode = 2;
+    ht.max_iter = std::max(1, cfg.h_cycle);
+  }
+  auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
+  omg->trace = c.trace_id(lv + ".OrthoMG");
+  omg->sweeps = std::max(1, cfg.h_sweeps);
+  omg->post = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
+  omg->post->trace = c.trace_id(lv + ".BlockJacobi");
+  const HmgLevel& L = H->levels[k];
+  auto tr = std::make_unique<TransferT<T>>(c, L.P.get(), L.R.get());
+  tr->trace = c.trace_id(lv + ".Transfer");
+  const Matrix* next64 = H->levels[k + 1].Aref;
+  tr->lower = build_hmg_level<T>(t, H, level_matrix<T>(t, next64), k + 1);
+  omg->coarse = std::move(tr);
+  return omg;
+}
+
 // A64: FP64 level operator (factorisations are computed from it); AT: the same operator in the precision T the
 // level runs in (AT == A64 for T = double).
 template <typename T>
@@ -814,6 +1038,23 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   const bsgpu_solver_config& cfg = t.cfg;
   Ctx& c = *t.ctx;
   if (level == cfg.n_levels - 1) {
+    if (cfg.coarse_kind == BSGPU_COARSE_HMG) {
+      require(t.info.hprol != nullptr && !t.info.hprol->empty() && t.info.top != nullptr,
+              "the h-multigrid coarse solve needs h-level prolongations (bsgpu_mgop_add_h_level)");
+      t.hmgs.emplace_back(hmg_setup(*A64, *t.info.top, t.info.L, cfg.level_keep[level], *t.info.hprol,
+                                    cfg.dense_limit, c.st));
+      return build_hmg_level<T>(t, t.hmgs.back().get(), AT, 0);
+    }
+    if (cfg.coarse_kind == BSGPU_COARSE_AMG) {
+      t.amgs.emplace_back(amg_setup(*A64, std::max(1, cfg.h_levels), cfg.dense_limit, c.st));
+      Term ct;
+      ct.mode = 1;
+      ct.tol = cfg.coarse_tol;
+      ct.max_iter = cfg.coarse_max_iter;
+      auto s = std::make_unique<AmgPcgT<T>>(t, t.amgs.back().get(), AT, std::max(1, cfg.h_sweeps), ct);
+      s->trace = c.trace_id("L" + std::to_string(level) + ".AmgPCG");
+      return s;
+    }
     if (cfg.h_levels > 0 && A64->uniform && A64->Np == 1) return build_hlevel<T>(t, A64, AT, 0);
     if (cfg.coarse_kind == BSGPU_COARSE_DENSE) {
       require(A64->uniform && A64->Np == 1, "the dense coarse solve needs a p = 0 last level", BSGPU_ERR_UNSUPPORTED);
@@ -857,7 +1098,7 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
 
 }  // namespace
 
-Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg) {
+Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info) {
   require(!A->single, "the solver operator must be FP64");
   require(cfg.n_levels >= 1 && cfg.n_levels <= 8, "n_levels must be in 1..8");
   auto t = std::make_unique<Tree>();
@@ -866,6 +1107,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg) {
   t->ctx->tracing = tr != nullptr && tr[0] != '\0' && tr[0] != '0';
   t->A = A;
   t->cfg = cfg;
+  t->info = info;
   Term top;
   top.mode = cfg.termination == BSGPU_TERM_RELATIVE ? 1 : 0;
   top.tol = cfg.tol;

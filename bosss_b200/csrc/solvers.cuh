@@ -6,6 +6,7 @@
 #include <memory>
 
 #include "aggregation.cuh"
+#include "amg.cuh"
 #include "blas1.cuh"
 #include "blockops.cuh"
 #include "matrix.cuh"
@@ -78,8 +79,12 @@ struct Term {
   std::pair<bool, bool> operator()(int iter, double R0, double R) const;
 };
 
-struct TreeConfig {
-  bsgpu_solver_config cfg;
+// What the MultigridOperator holds beyond the transformed matrix: the untransformed finest matrix, its left
+// change of basis and the caller's h-level prolongations (used by the h-multigrid coarse solve).
+struct OperatorInfo {
+  const Matrix* top = nullptr;
+  const double* L = nullptr;  // device, per block row I x I row-major; nullptr for Eye
+  const std::vector<HostBsr>* hprol = nullptr;
 };
 
 // Builds the solver tree for `cfg` on the (transformed) operator A (FP64).  For BSGPU_PRECISION_MIXED the
@@ -88,10 +93,13 @@ struct Tree {
   std::unique_ptr<Ctx> ctx;
   std::vector<std::unique_ptr<Matrix>> owned;
   std::vector<std::unique_ptr<Aggregation>> aggs;
+  std::vector<std::unique_ptr<AmgHierarchy>> amgs;
+  std::vector<std::unique_ptr<HmgHierarchy>> hmgs;
   std::unique_ptr<Solver<double>> top;
   const Matrix* A = nullptr;
   bsgpu_solver_config cfg{};
+  OperatorInfo info;
 };
-Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg);
+Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info);
 
 }  // namespace bsgpu

@@ -15,7 +15,7 @@ HOST_POINTERS, DEVICE_POINTERS = 0, 1
 COB_EYE, COB_DIAG_BLOCK_EQUILIB = 0, 1
 SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI = 0, 1, 2, 3
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
-COARSE_DENSE, COARSE_PCG = 0, 1
+COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 
 # every symbol the header declares (checked by the CPU test-suite)
@@ -25,7 +25,8 @@ EXPORTS = [
     "bsgpu_matrix_spmv", "bsgpu_matrix_spmv_noalloc", "bsgpu_matrix_spmv_device", "bsgpu_matrix_create_single",
     "bsgpu_matrix_spmv_device_f32",
     "bsgpu_matrix_restrict",
-    "bsgpu_mgop_create", "bsgpu_mgop_destroy", "bsgpu_mgop_get_operator", "bsgpu_mgop_read_left_cob",
+    "bsgpu_mgop_create", "bsgpu_mgop_destroy", "bsgpu_mgop_get_operator", "bsgpu_mgop_add_h_level",
+    "bsgpu_mgop_read_left_cob",
     "bsgpu_solver_config_default", "bsgpu_solver_create", "bsgpu_solver_destroy", "bsgpu_solver_solve",
     "bsgpu_solver_solve_device", "bsgpu_solver_get_history", "bsgpu_solver_set_tracing", "bsgpu_solver_get_trace",
 ]
@@ -89,6 +90,7 @@ def lib() -> C.CDLL:
             "bsgpu_mgop_destroy": [vp],
             "bsgpu_mgop_get_operator": [vp, vp],
             "bsgpu_mgop_read_left_cob": [vp, vp],
+            "bsgpu_mgop_add_h_level": [vp, i32, i64, i64, vp, vp, vp],
             "bsgpu_solver_config_default": [vp],
             "bsgpu_solver_create": [vp, vp, vp],
             "bsgpu_solver_destroy": [vp],

@@ -139,7 +139,9 @@ class MultigridOperator:
 
     Eye, DiagBlockEquilib = nat.COB_EYE, nat.COB_DIAG_BLOCK_EQUILIB
 
-    def __init__(self, A: BlockMsrMatrix, mode: int = nat.COB_DIAG_BLOCK_EQUILIB):
+    def __init__(self, A: BlockMsrMatrix, mode: int = nat.COB_DIAG_BLOCK_EQUILIB, h_levels=()):
+        """``h_levels``: prolongations of the agglomeration levels below the coarsest p-level, finest first
+        (objects with Np, nb_fine, nb_coarse, row_ptr, col_idx, values -- e.g. ``assembly.h_hierarchy``)."""
         self.BaseMatrix = A
         self.mode = mode
         h = C.c_void_p()
@@ -148,6 +150,15 @@ class MultigridOperator:
         oh = C.c_void_p()
         nat.check(nat.lib().bsgpu_mgop_get_operator(self._h, C.byref(oh)))
         self.OperatorMatrix = BlockMsrMatrix(oh, owner=False)
+        for P in h_levels:
+            self.AddHLevel(P)
+
+    def AddHLevel(self, P):
+        rp = np.ascontiguousarray(P.row_ptr, np.int64)
+        ci = np.ascontiguousarray(P.col_idx, np.int32)
+        v = np.ascontiguousarray(P.values, np.float64)
+        nat.check(nat.lib().bsgpu_mgop_add_h_level(self._h, int(P.Np), int(P.nb_fine), int(P.nb_coarse),
+                                                   nat.ptr(rp), nat.ptr(ci), nat.ptr(v)))
 
     def LeftChangeOfBasis(self, total_len: int) -> np.ndarray:
         out = np.empty(total_len)
@@ -192,8 +203,13 @@ class PmgConfig(IterativeSolverConfig):
     """PmgConfig.CreateInstanceImpl__Kummer with UseILU = false (block-Jacobi post-smoother on every level).
 
     ``DegreeHierarchy``: modes per species kept on each level, finest first (e.g. (20, 10, 4) for p = 3 -> 2 -> 1
-    in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative), or densely
-    (``CoarseSolver = "dense"``, p = 0 levels up to 4096 unknowns).  With ``HLevels > 0`` and a p = 0 last level
+    in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative), by CG
+    preconditioned with a smoothed-aggregation AMG V-cycle (``CoarseSolver = "amg"``: ``HLevels`` AMG levels,
+    ``HSweeps`` Jacobi sweeps, dense below ``DenseLimit``), or densely (``CoarseSolver = "dense"``, p = 0 levels
+    up to 4096 unknowns), or by h-multigrid on the agglomeration levels given to the ``MultigridOperator``
+    (``CoarseSolver = "hmg"``: OrthoMG to ``CoarseTolerance`` with ``HSweeps`` block-Jacobi sweeps,
+    ``HCycle`` iterations per coarser h-level, dense below ``DenseLimit``).
+    With ``HLevels > 0``, ``CoarseSolver = "pcg"`` and a p = 0 last level
     (DegreeHierarchy ending in 1), up to ``HLevels`` aggregation h-levels follow, each an OrthoMG with
     ``HCycle`` iterations and ``HSweeps`` post-smoother sweeps, down to ``DenseLimit`` unknowns.
     """
@@ -221,7 +237,10 @@ class PmgConfig(IterativeSolverConfig):
         c.post_sweeps = self.NoOfPostSmootherSweeps
         c.bj_iters = self.BlockJacobiIterations
         c.bj_omega = self.BlockJacobiOmega
-        c.coarse_kind = nat.COARSE_DENSE if self.CoarseSolver == "dense" else nat.COARSE_PCG
+        kinds = {"dense": nat.COARSE_DENSE, "pcg": nat.COARSE_PCG, "amg": nat.COARSE_AMG, "hmg": nat.COARSE_HMG}
+        if self.CoarseSolver not in kinds:
+            raise ValueError(f"CoarseSolver must be one of {sorted(kinds)}")
+        c.coarse_kind = kinds[self.CoarseSolver]
         c.coarse_tol = self.CoarseTolerance
         c.coarse_max_iter = self.CoarseMaxIterations
         c.sub_max_iter = self.SubLevelMaxIterations

@@ -103,6 +103,13 @@ BSGPU_API int bsgpu_mgop_create(bsgpu_mgop_t* op, bsgpu_matrix_t A, int32_t mode
 BSGPU_API int bsgpu_mgop_destroy(bsgpu_mgop_t op);
 /* Borrowed handle of the transformed operator (owned by op). */
 BSGPU_API int bsgpu_mgop_get_operator(bsgpu_mgop_t op, bsgpu_matrix_t* Aop);
+/* Adds one h-level below the coarsest p-level, finest first: the prolongation from the agglomerated (coarser)
+ * grid to the current one, in the untransformed orthonormal DG basis of that p-level, as block-CSR with
+ * nb_fine block rows, nb_coarse block columns and Np x Np row-major blocks (host pointers).  The counterpart of
+ * the prolongation operators of the reference's multigrid hierarchy on aggregation grids
+ * (MultigridOperator.cs:774,815; AggregationGridBasis.cs); used by BSGPU_COARSE_HMG. */
+BSGPU_API int bsgpu_mgop_add_h_level(bsgpu_mgop_t op, int32_t Np, int64_t nb_fine, int64_t nb_coarse,
+                                     const int64_t* row_ptr, const int32_t* col_idx, const double* values);
 /* Per-block L factors, row-major, concatenated in block order (host buffer). */
 BSGPU_API int bsgpu_mgop_read_left_cob(bsgpu_mgop_t op, double* L);
 
@@ -114,7 +121,12 @@ enum {
   BSGPU_SOLVER_BLOCKJACOBI = 3  /* BlockJacobi.cs:35 as a standalone smoother                               */
 };
 enum { BSGPU_TERM_DEFAULT = 0 /* R < R0*tol + tol */, BSGPU_TERM_RELATIVE = 1 /* R < R0*tol */ };
-enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1 };
+/* coarsest-level solver: dense inverse (p = 0, <= 4096 unknowns), block-Jacobi PCG, or PCG preconditioned by a
+ * smoothed-aggregation AMG V-cycle (h_levels levels, h_sweeps Jacobi sweeps, dense below dense_limit) */
+enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1, BSGPU_COARSE_AMG = 2,
+       BSGPU_COARSE_HMG = 3 /* h-multigrid on the caller's agglomeration levels (bsgpu_mgop_add_h_level):
+                               OrthoMG to coarse_tol with h_sweeps block-Jacobi sweeps, h_cycle iterations on the
+                               coarser h-levels, dense below dense_limit */ };
 enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in FP32, outer FP64 */ };
 
 typedef struct {

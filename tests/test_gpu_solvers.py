@@ -130,6 +130,48 @@ def test_fgmres_pmg_with_h_levels(cuda, mixed):
     assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_fgmres_pmg_with_amg_coarse(cuda, mixed):
+    """p-levels 3 -> 2 -> 1; the p = 1 level solved by CG + smoothed-aggregation AMG."""
+    s = A.poisson_3d(10, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseSolver="amg", HLevels=4, HSweeps=2, DenseLimit=64,
+                    CoarseTolerance=1e-3)
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
+                       MixedPrecision=mixed).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged and slv.ThisLevelIterations < 40
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_fgmres_pmg_with_h_multigrid_coarse(cuda, mixed):
+    """p-levels 3 -> 2 -> 1; the p = 1 level solved by h-multigrid on 2x2x2 agglomerations (16^3 -> 8^3 -> 4^3)."""
+    s = A.poisson_3d(16, 3)
+    hl = A.h_hierarchy(s.grid, 1)
+    assert [P.nb_coarse for P in hl] == [512, 64]
+    op = MultigridOperator(BlockMsrMatrix.from_system(s), h_levels=hl)
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseSolver="hmg", HSweeps=3, HCycle=1, CoarseTolerance=1e-2,
+                    DenseLimit=256)
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
+                       MixedPrecision=mixed).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged and slv.ThisLevelIterations < 40
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+def test_h_multigrid_needs_prolongations(cuda):
+    s = A.poisson_3d(4, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseSolver="hmg")
+    with pytest.raises(ValueError):
+        FGMRESConfig(Preconditioners=[pmg]).CreateInstance(op)
+
+
 def test_dense_coarse_solve(cuda):
     s = A.poisson_3d(4, 2)
     op = MultigridOperator(BlockMsrMatrix.from_system(s))
