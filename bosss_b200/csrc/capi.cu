@@ -35,6 +35,8 @@ thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 static std::atomic<unsigned long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void add_launches(long long n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+unsigned long long launches_now() { return g_launches.load(); }
 const Matrix* matrix_from_handle(bsgpu_matrix_t A) { return A ? A->get() : nullptr; }
 
 namespace {

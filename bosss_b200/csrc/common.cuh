@@ -37,6 +37,9 @@ void set_last_error(const std::string& msg);
 // Every kernel launch of the library is followed by this check, which also counts the launch (the count is
 // exposed through bsgpu_get_launch_count for tracing).
 void count_launch();
+// Adjusts the counter for graph capture (kernels recorded into a graph run when the graph is replayed).
+void add_launches(long long n);
+unsigned long long launches_now();
 #define BSGPU_CHECK_LAUNCH()          \
   do {                                \
     BSGPU_CUDA(cudaGetLastError());   \

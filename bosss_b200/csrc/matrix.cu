@@ -96,16 +96,22 @@ struct Acc { using type = T; };
 template <typename T, int NP, int V, int MODE>
 __global__ void __launch_bounds__(256) spmv_uniform_kernel(
     const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const T* __restrict__ vals,
-    const T* __restrict__ x, const T* __restrict__ z, T* __restrict__ y, T alpha, T beta, int64_t nb,
-    const T* __restrict__ dinv, const int* __restrict__ active) {
+    const T* x, const T* __restrict__ z, T* y, T alpha, T beta, int64_t nb,
+    const T* __restrict__ dinv, const int* __restrict__ active, const int32_t* __restrict__ row_list = nullptr) {
   constexpr int BPC = 256 / NP;
   static_assert(NP % V == 0, "chunk width must divide the block size");
   if (active != nullptr && *active == 0) return;
   const int t = threadIdx.x;
   const int lb = t / NP;
   const int r = t - lb * NP;
-  const int64_t i = (int64_t)blockIdx.x * BPC + lb;
-  const bool valid = (lb < BPC) && (i < nb);
+  // MODE 2 (block Gauss-Seidel half-sweep): the block rows come from `row_list` (one colour; nb is the list
+  // length) and the update is in place (x == y): all reads of x precede the barrier, the write follows it, and
+  // no block row of the list reads another row of the list.
+  int64_t i = (int64_t)blockIdx.x * BPC + lb;
+  bool valid = (lb < BPC) && (i < nb);
+  if constexpr (MODE == 2) {
+    if (valid) i = row_list[i];
+  }
   const uint64_t pol = policy_evict_first();
   T acc0 = 0, acc1 = 0;
   if (valid) {
@@ -560,6 +566,58 @@ void bj_update_impl(const Matrix& A, const T* vals, const T* dinv, T omega, cons
   dispatch<T, 1>(A, vals, x, b, xo, omega, T(0), dinv, A.doff.p, st, active);
 }
 }  // namespace
+
+namespace {
+template <typename T>
+void gs_rows_impl(const Matrix& A, const T* vals, const T* dinv, T omega, const int32_t* rows, int64_t nrows,
+                  const T* b, T* x, cudaStream_t st) {
+  require(specialised(A), "block Gauss-Seidel needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
+  if (nrows == 0) return;
+  constexpr int VW = sizeof(T) == 8 ? 2 : 4;
+#define BSGPU_GS(NP, VV)                                                                                     \
+  spmv_uniform_kernel<T, NP, VV, 2><<<(unsigned)((nrows + 256 / NP - 1) / (256 / NP)), (256 / NP) * NP, 0, st>>>( \
+      A.rp.p, A.ci.p, vals, x, b, x, omega, T(0), nrows, dinv, nullptr, rows)
+  switch (A.Np) {
+    case 20: BSGPU_GS(20, VW); break;
+    case 4: BSGPU_GS(4, VW); break;
+    case 10: BSGPU_GS(10, 2); break;
+    case 6: BSGPU_GS(6, 2); break;
+  }
+#undef BSGPU_GS
+  BSGPU_CHECK_LAUNCH();
+}
+}  // namespace
+
+void gs_update_rows(const Matrix& A, const double* dinv, double omega, const int32_t* rows, int64_t nrows,
+                    const double* b, double* x, cudaStream_t st) {
+  require(!A.single, "precision mismatch");
+  gs_rows_impl<double>(A, A.v64.p, dinv, omega, rows, nrows, b, x, st);
+}
+void gs_update_rows(const Matrix& A, const float* dinv, float omega, const int32_t* rows, int64_t nrows,
+                    const float* b, float* x, cudaStream_t st) {
+  require(A.single, "precision mismatch");
+  gs_rows_impl<float>(A, A.v32.p, dinv, omega, rows, nrows, b, x, st);
+}
+
+std::vector<std::vector<int32_t>> greedy_colouring(const Matrix& A) {
+  std::vector<int32_t> col(A.nb, -1);
+  int ncol = 0;
+  std::vector<char> used;
+  for (int64_t i = 0; i < A.nb; ++i) {
+    used.assign(ncol + 1, 0);
+    for (int64_t k = A.h_rp[i]; k < A.h_rp[i + 1]; ++k) {
+      const int32_t j = A.h_ci[k];
+      if (j != i && col[j] >= 0) used[col[j]] = 1;
+    }
+    int c = 0;
+    while (c < ncol && used[c]) ++c;
+    col[i] = c;
+    if (c == ncol) ++ncol;
+  }
+  std::vector<std::vector<int32_t>> lists(ncol);
+  for (int64_t i = 0; i < A.nb; ++i) lists[col[i]].push_back((int32_t)i);
+  return lists;
+}
 
 void bj_update(const Matrix& A, const double* dinv, double omega, const double* x, const double* b, double* xo,
                cudaStream_t st, const int* active) {

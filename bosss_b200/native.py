@@ -17,6 +17,7 @@ SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI = 0, 1, 2,
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS = 0, 1
 
 # every symbol the header declares (checked by the CPU test-suite)
 EXPORTS = [
@@ -39,7 +40,8 @@ class SolverConfig(C.Structure):
                 ("bj_omega", C.c_double), ("coarse_kind", C.c_int32), ("coarse_tol", C.c_double),
                 ("coarse_max_iter", C.c_int32), ("sub_max_iter", C.c_int32), ("sub_reduction", C.c_double),
                 ("precision", C.c_int32), ("h_levels", C.c_int32), ("h_sweeps", C.c_int32), ("h_cycle", C.c_int32),
-                ("dense_limit", C.c_int32), ("reserved", C.c_int32 * 12)]
+                ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
+                ("reserved", C.c_int32 * 10)]
 
 
 class SolveStats(C.Structure):

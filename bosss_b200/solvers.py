@@ -226,6 +226,8 @@ class PmgConfig(IterativeSolverConfig):
     HSweeps: int = 3
     HCycle: int = 1
     DenseLimit: int = 1024
+    Smoother: str = "blockjacobi"
+    HSmoother: str = "blockjacobi"
     UseILU: bool = False
 
     def _fill(self, c):
@@ -249,6 +251,11 @@ class PmgConfig(IterativeSolverConfig):
         c.h_sweeps = self.HSweeps
         c.h_cycle = self.HCycle
         c.dense_limit = self.DenseLimit
+        sm = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "blockgs": nat.SMOOTHER_BLOCKGS}
+        if self.Smoother not in sm or self.HSmoother not in sm:
+            raise ValueError(f"Smoother / HSmoother must be one of {sorted(sm)}")
+        c.smoother = sm[self.Smoother]
+        c.h_smoother = sm[self.HSmoother]
 
     def _config(self):
         c = self._base()

@@ -128,6 +128,9 @@ enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1, BSGPU_COARSE_AMG = 2,
                                OrthoMG to coarse_tol with h_sweeps block-Jacobi sweeps, h_cycle iterations on the
                                coarser h-levels, dense below dense_limit */ };
 enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in FP32, outer FP64 */ };
+/* post-smoother of the OrthoMG levels: BlockJacobi (BlockJacobi.cs:35; NoOfIterations = bj_iters), or symmetric
+ * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20) */
+enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1 };
 
 typedef struct {
   int32_t solver;           /* BSGPU_SOLVER_*                                                   */
@@ -151,7 +154,9 @@ typedef struct {
   int32_t h_sweeps;         /* post-smoother sweeps on the h-levels                             */
   int32_t h_cycle;          /* OrthoMG iterations per call on the h-levels (1 = V-cycle)        */
   int32_t dense_limit;      /* levels with at most this many unknowns are solved densely        */
-  int32_t reserved[12];
+  int32_t smoother;         /* BSGPU_SMOOTHER_* on the p-levels                                 */
+  int32_t h_smoother;       /* BSGPU_SMOOTHER_* on the h-levels (aggregation / h-multigrid)     */
+  int32_t reserved[10];
 } bsgpu_solver_config;
 
 typedef struct {

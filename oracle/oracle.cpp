@@ -833,6 +833,69 @@ int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const do
   }
 }
 
+// Persistent solver: set-up once (level matrices, block inverses), solve many times.
+struct or_solver_s {
+  Mat A;
+  Solver* s = nullptr;
+  std::vector<Restriction*> keep;
+  std::vector<double> hist;
+  ~or_solver_s() { delete s; }
+};
+
+or_solver_t or_solver_create(const or_bsr* m, const or_solver_cfg* c) {
+  try {
+    auto* h = new or_solver_s();
+    load_mat(h->A, m);
+    Term top;
+    top.mode = c->top_mode;
+    top.tol = c->tol;
+    top.max_iter = c->max_iter;
+    top.min_iter = c->min_iter;
+    if (c->solver == OR_SOLVER_FGMRES_PMG) {
+      or_solver_cfg pc = *c;
+      pc.top_mode = 2;
+      pc.max_iter = 1;
+      Solver* prec = build_level(&h->A, &pc, 0, h->keep);
+      auto* f = new FlexGMRES(&h->A, prec, c->max_krylov, top);
+      f->reference_defect = c->reference_fgmres_defect != 0;
+      f->hist = &h->hist;
+      h->s = f;
+    } else if (c->solver == OR_SOLVER_ORTHOMG) {
+      h->s = build_level(&h->A, c, 0, h->keep);
+    } else {
+      h->s = new SoftPCG(&h->A, c->bj_iters >= 0 ? new BlockJacobi(&h->A, c->bj_iters, c->bj_omega) : nullptr, top);
+    }
+    return h;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return nullptr;
+  }
+}
+
+int or_solver_solve(or_solver_t h, const double* b, double* x, or_stats* stats) {
+  try {
+    Vec X(x, x + h->A.N), B(b, b + h->A.N);
+    h->hist.clear();
+    h->s->this_level_iterations = 0;
+    h->s->solve(X, B);
+    std::copy(X.begin(), X.end(), x);
+    if (stats) {
+      stats->iterations = h->s->this_level_iterations;
+      stats->nested = h->s->nested();
+      stats->converged = h->s->converged ? 1 : 0;
+      stats->n_hist = (int)h->hist.size();
+      stats->res0 = h->hist.empty() ? 0 : h->hist.front();
+      stats->res = h->hist.empty() ? 0 : h->hist.back();
+    }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return OR_ERR_ARITHMETIC;
+  }
+}
+
+void or_solver_destroy(or_solver_t h) { delete h; }
+
 int or_solve(const or_bsr* m, const or_solver_cfg* c, const double* b, double* x, or_stats* stats,
              double* hist, int hist_cap) {
   try {

@@ -51,4 +51,9 @@ int or_restrict(const or_bsr* m, int keep, double* values_out, int64_t* map_out)
 int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const double* b);
 int or_solve(const or_bsr* m, const or_solver_cfg* c, const double* b, double* x, or_stats* stats, double* hist,
              int hist_cap);
+/* persistent solver (set-up once, many solves); the matrix arrays must outlive it */
+typedef struct or_solver_s* or_solver_t;
+or_solver_t or_solver_create(const or_bsr* m, const or_solver_cfg* c);
+int or_solver_solve(or_solver_t h, const double* b, double* x, or_stats* stats);
+void or_solver_destroy(or_solver_t h);
 #endif

@@ -213,6 +213,38 @@ def solve(A: Bsr, b: np.ndarray, cfg: SolverConfig, x0: np.ndarray | None = None
                        res0=st.res0, res=st.res, history=hist[:min(st.n_hist, cap)].copy())
 
 
+class PersistentSolver:
+    """Set-up once (level matrices, block inverses), then time only the solves."""
+
+    def __init__(self, A: Bsr, cfg: SolverConfig):
+        L = lib()
+        L.or_solver_create.restype = C.c_void_p
+        L.or_solver_create.argtypes = [C.c_void_p, C.c_void_p]
+        L.or_solver_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_solver_destroy.argtypes = [C.c_void_p]
+        self.A = A
+        self._cfg = cfg._c()
+        self._h = L.or_solver_create(C.byref(A._c), C.byref(self._cfg))
+        if not self._h:
+            raise ArithmeticError(f"oracle set-up failed: {L.or_last_error().decode()}")
+
+    def solve(self, b: np.ndarray, x0: np.ndarray | None = None) -> SolveResult:
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.A.N) if x0 is None else np.ascontiguousarray(x0, np.float64).copy()
+        st = _Stats()
+        _check(lib().or_solver_solve(self._h, b.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p),
+                                     C.byref(st)))
+        return SolveResult(x=x, iterations=st.iterations, nested=st.nested, converged=bool(st.converged),
+                           res0=st.res0, res=st.res, history=np.zeros(0))
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().or_solver_destroy(self._h)
+        except Exception:
+            pass
+
+
 def direct_solve(system, rhs=None) -> np.ndarray:
     """FP64 sparse direct solve (scipy SuperLU) -- the exact-solution oracle for small systems."""
     import scipy.sparse.linalg as spla

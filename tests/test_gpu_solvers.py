@@ -136,7 +136,7 @@ def test_fgmres_pmg_with_amg_coarse(cuda, mixed):
     s = A.poisson_3d(10, 3)
     op = MultigridOperator(BlockMsrMatrix.from_system(s))
     pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseSolver="amg", HLevels=4, HSweeps=2, DenseLimit=64,
-                    CoarseTolerance=1e-3)
+                    CoarseTolerance=1e-1, CoarseMaxIterations=30)
     slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
                        MixedPrecision=mixed).CreateInstance(op)
     x = np.zeros(s.N)
@@ -153,8 +153,8 @@ def test_fgmres_pmg_with_h_multigrid_coarse(cuda, mixed):
     hl = A.h_hierarchy(s.grid, 1)
     assert [P.nb_coarse for P in hl] == [512, 64]
     op = MultigridOperator(BlockMsrMatrix.from_system(s), h_levels=hl)
-    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseSolver="hmg", HSweeps=3, HCycle=1, CoarseTolerance=1e-2,
-                    DenseLimit=256)
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseSolver="hmg", HSweeps=2, HCycle=1, CoarseTolerance=1e-1,
+                    CoarseMaxIterations=20, DenseLimit=256, HSmoother="blockgs")
     slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
                        MixedPrecision=mixed).CreateInstance(op)
     x = np.zeros(s.N)
@@ -223,3 +223,18 @@ def test_nan_rhs_raises_arithmetic_error(cuda):
     b[5] = np.nan
     with pytest.raises(ArithmeticError):
         slv.Solve(np.zeros(s.N), b)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_block_gauss_seidel_smoother(cuda, mixed):
+    """Symmetric multicolour block Gauss-Seidel on the p-levels, capped PCG coarse solve."""
+    s = A.poisson_3d(8, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), Smoother="blockgs", CoarseTolerance=1e-1, CoarseMaxIterations=40)
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
+                       MixedPrecision=mixed).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
