@@ -136,6 +136,20 @@ class RectilinearGrid:
             out.append(0.5 * (n[:-1] + n[1:])[mi[d]])
         return out
 
+    def face_neighbours(self) -> np.ndarray:
+        """[cells, 2D] neighbour ids in the order -x, +x, -y, +y, -z, +z (-1 on the boundary)."""
+        mi = self.cell_multi_index()
+        ids = np.arange(self.ncells, dtype=np.int64)
+        out = np.full((self.ncells, 2 * self.D), -1, dtype=np.int32)
+        stride = 1
+        for d in range(self.D):
+            lo = mi[d] > 0
+            hi = mi[d] < self.shape[d] - 1
+            out[lo, 2 * d] = (ids[lo] - stride).astype(np.int32)
+            out[hi, 2 * d + 1] = (ids[hi] + stride).astype(np.int32)
+            stride *= self.shape[d]
+        return out
+
     def length_scale_cj(self) -> np.ndarray:
         """cj = 0.5 * (surface + boundary area) / volume, per cell (GridData_CellData.cs:681-687)."""
         hs = self.cell_sizes()

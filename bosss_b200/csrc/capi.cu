@@ -18,6 +18,9 @@ struct bsgpu_mgop_s {
   int mode = 0;
   bsgpu_matrix_s op_handle;    // borrowed handle returned by bsgpu_mgop_get_operator
   std::vector<bsgpu::HostBsr> hprol;  // h-level prolongations below the coarsest p-level
+  int nfaces = 0, nfeat = 0;          // cell graph and features for the learned stage
+  std::vector<int32_t> nbr;
+  std::vector<float> feats;
   const bsgpu::Matrix* op() const { return mode == BSGPU_COB_EYE ? A : Aop.get(); }
 };
 
@@ -286,6 +289,24 @@ BSGPU_API int bsgpu_mgop_add_h_level(bsgpu_mgop_t op, int32_t Np, int64_t nb_fin
   });
 }
 
+BSGPU_API int bsgpu_mgop_set_cell_neighbours(bsgpu_mgop_t op, int32_t nfaces, const int32_t* nbr) {
+  return guarded([&] {
+    require(op && nbr && nfaces > 0 && nfaces <= 16, "bad cell neighbour table");
+    const int64_t nb = op->A->nb;
+    for (int64_t i = 0; i < nb * nfaces; ++i) require(nbr[i] >= -1 && nbr[i] < nb, "neighbour index out of range");
+    op->nfaces = nfaces;
+    op->nbr.assign(nbr, nbr + nb * nfaces);
+  });
+}
+
+BSGPU_API int bsgpu_mgop_set_cell_features(bsgpu_mgop_t op, int32_t nfeat, const float* feats) {
+  return guarded([&] {
+    require(op && (feats || nfeat == 0) && nfeat >= 0 && nfeat <= 64, "bad cell feature table");
+    op->nfeat = nfeat;
+    op->feats.assign(feats, feats + op->A->nb * (int64_t)nfeat);
+  });
+}
+
 BSGPU_API int bsgpu_mgop_read_left_cob(bsgpu_mgop_t op, double* L) {
   return guarded([&] {
     require(op && L, "null argument");
@@ -319,6 +340,9 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->h_sweeps = 3;
     cfg->h_cycle = 1;
     cfg->dense_limit = 1024;
+    cfg->learned = BSGPU_LEARNED_OFF;
+    cfg->learned_hidden = 64;
+    cfg->learned_stall = 0.99;
   });
 }
 
@@ -331,6 +355,10 @@ BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgp
     info.top = op->A;
     info.L = op->mode == BSGPU_COB_DIAG_BLOCK_EQUILIB ? op->L.p : nullptr;
     info.hprol = &op->hprol;
+    info.nfaces = op->nfaces;
+    info.nbr = op->nfaces ? &op->nbr : nullptr;
+    info.nfeat = op->nfeat;
+    info.feats = op->nfeat ? &op->feats : nullptr;
     h->tree.reset(build_tree(op->op(), *cfg, info));
     const int64_t N = std::max<int64_t>(op->A->N, 1);
     h->X.alloc(N); h->B.alloc(N); h->Xt.alloc(N); h->Bt.alloc(N);
@@ -371,6 +399,15 @@ BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const doubl
     require(s && X && B, "null argument");
     BSGPU_CUDA(cudaDeviceSynchronize());
     solve_device(s, X, B, stats);
+  });
+}
+
+BSGPU_API int bsgpu_solver_train_learned(bsgpu_solver_t s, int32_t n_rhs, int32_t steps, double lr, uint64_t seed,
+                                         double* loss) {
+  return guarded([&] {
+    require(s != nullptr, "null solver");
+    const double l = train_learned(*s->tree, n_rhs, steps, lr, seed);
+    if (loss) *loss = l;
   });
 }
 

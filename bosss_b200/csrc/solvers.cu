@@ -512,7 +512,8 @@ template <typename T>
 struct OrthoMGT : Solver<T> {
   const Matrix* A;
   int64_t N;
-  std::unique_ptr<Solver<T>> coarse, post;
+  std::unique_ptr<Solver<T>> coarse, post, pre;
+  const bool* pre_on = nullptr;  // the pre-smoother runs only while *pre_on (learned stage trained)
   int sweeps = 10;
   Term term;
   OrthoT<T> ortho;
@@ -549,6 +550,18 @@ struct OrthoMGT : Solver<T> {
         // history capacity reached: restart the minimisation from the current iterate
         copy_vec(Res0.p, Res.p, N, c.st);
         ortho.clear();
+      }
+      if (pre && (pre_on == nullptr || *pre_on)) {
+        // pre-smoother (OrthonormalizationMultigrid.cs:893-915)
+        T* pc = ortho.next_sol(c);
+        pre->solve(c, pc, Res.p, true);
+        ortho.add_sol(c);
+        rn = ortho.minimize(c, X, B, Res0.p, Res.p, rn);
+        st = term(iIter, r0, rn);
+        if (!st.first) {
+          this->converged = st.second;
+          break;
+        }
       }
       if (coarse) {
         T* vl = ortho.next_sol(c);
@@ -858,6 +871,25 @@ struct AmgPcgT : Solver<T> {
   }
 };
 
+// The learned stage as a preconditioner / smoother: X = NN(B) (learned.cu); inputs normalised by the RMS of B.
+template <typename T>
+struct LearnedPrecondT : Solver<T> {
+  const LearnedNet* net;
+  int64_t N;
+  double* d_s;  // [0] |B|, [1] scale
+  LearnedPrecondT(Ctx& c, const LearnedNet* n_) : net(n_), N(n_->ncells * n_->Np) { d_s = c.scal(2); }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    (void)zero;
+    const T* a[1] = {B};
+    dots(c.red, 1, a, a, N, d_s, 1, c.st);
+    learned_scale(d_s, d_s + 1, N, c.st);
+    learned_apply(*net, B, X, d_s + 1, c.st);
+    this->converged = true;
+    this->this_level_iterations = 1;
+  }
+};
+
 // FP64 interface around an FP32 solver (mixed-precision preconditioner).
 struct MixedAdapter : Solver<double> {
   std::unique_ptr<Solver<float>> inner;
@@ -895,6 +927,11 @@ struct FlexGMRES : Solver<double> {
   int m;
   Term term;
   std::unique_ptr<Solver<double>> pc;
+  // second preconditioner used in turn with pc (FlexGMRES.cs:196-199 cycles PrecondS); switched off for the rest
+  // of a solve when one of its steps reduces the residual estimate by less than the factor `stall`
+  std::unique_ptr<Solver<double>> pc2;
+  Tree* tree = nullptr;
+  double stall = 0.99;
   std::vector<DBuf<double>> V, Z;
   DBuf<double> R0;
   double* d_h;     // [2*(m+1)] projections of both sweeps
@@ -931,6 +968,8 @@ struct FlexGMRES : Solver<double> {
   void solve(Ctx& c, double* X, const double* B, bool zero) override {
     TraceScope ts(c, this->trace);
     std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    bool nn_active = pc2 && tree && tree->learned_on;
+    int turn = 0;
     int iIter = 0;
     double r0 = 0;
     this->history.clear();
@@ -958,7 +997,12 @@ struct FlexGMRES : Solver<double> {
       int j;
       for (j = 0; j < m; ++j) {
         fill(0.0, Z[j].p, N, c.st);
-        pc->solve(c, Z[j].p, V[j].p, true);
+        const bool use2 = pc2 && nn_active && (turn++ % 2 == 1);
+        const double g_before = std::fabs(g[j]);
+        if (use2)
+          pc2->solve(c, Z[j].p, V[j].p, true);
+        else
+          pc->solve(c, Z[j].p, V[j].p, true);
         iIter++;
         double* W = V[j + 1].p;
         spmv(*A, 1.0, Z[j].p, 0.0, (const double*)nullptr, W, c.st);
@@ -973,6 +1017,10 @@ struct FlexGMRES : Solver<double> {
         for (int i = 0; i <= j; ++i) H[i * m + j] = hh[i] + hh[m + 1 + i];
         H[(j + 1) * m + j] = wn;
         if (wn > 0) axpby(1.0 / wn, W, 0.0, W, N, c.st);
+        if (tree && tree->collect && tree->collect->size() < tree->collect_cap && wn > 0) {
+          tree->collect->emplace_back(N);
+          copy_vec(tree->collect->back().p, (const double*)W, N, c.st);
+        }
         for (int i = 0; i < j; ++i) {
           const double a0 = H[i * m + j], b0 = H[(i + 1) * m + j];
           H[i * m + j] = cs[i] * a0 + sn[i] * b0;
@@ -988,6 +1036,10 @@ struct FlexGMRES : Solver<double> {
         g[j] = cs[j] * g[j];
         const double est = std::fabs(g[j + 1]);
         this->history.push_back(est);
+        if (use2 && est > stall * g_before) {
+          nn_active = false;  // the learned stage stalls: plain p-multigrid for the rest of this solve
+          if (tree) tree->learned_stalls++;
+        }
         auto st2 = term(iIter, r0, est);
         if (!st2.first || st2.second || wn == 0.0) {
           ++j;
@@ -1174,6 +1226,11 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   const std::string lv = "L" + std::to_string(level);
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
   omg->trace = c.trace_id(lv + ".OrthoMG");
+  if (level == 0 && t.net && (cfg.learned & BSGPU_LEARNED_PRESMOOTH)) {
+    omg->pre = std::make_unique<LearnedPrecondT<T>>(c, t.net.get());
+    omg->pre->trace = c.trace_id(lv + ".LearnedPreSmoother");
+    omg->pre_on = &t.learned_on;
+  }
   omg->sweeps = cfg.post_sweeps;
   omg->post = make_smoother<T>(c, A64, AT, cfg.smoother, cfg, lv);
   const int keep = cfg.level_keep[level + 1];
@@ -1210,6 +1267,20 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
       require(cfg.level_keep[l] >= 1 && cfg.level_keep[l] < cfg.level_keep[l - 1], "level_keep must decrease");
   }
   const bool mixed = cfg.precision == BSGPU_PRECISION_MIXED;
+  if (cfg.learned != BSGPU_LEARNED_OFF) {
+    require(cfg.solver == BSGPU_SOLVER_FGMRES_PMG, "the learned stage needs the FGMRES + p-multigrid solver");
+    require(info.nbr != nullptr && info.nfaces > 0, "the learned stage needs the cell graph (bsgpu_mgop_set_cell_neighbours)");
+    require(A->uniform, "the learned stage needs one species per cell", BSGPU_ERR_UNSUPPORTED);
+    require((int64_t)info.nbr->size() == A->nb * info.nfaces, "cell neighbour table size mismatch");
+    if (info.nfeat) require((int64_t)info.feats->size() == A->nb * info.nfeat, "cell feature table size mismatch");
+    t->net = std::make_unique<LearnedNet>();
+    if (cfg.learned_hidden > 0) {
+      require(cfg.learned_hidden % 16 == 0 && cfg.learned_hidden <= 128, "learned_hidden must be a multiple of 16, <= 128");
+      t->net->H = cfg.learned_hidden;
+    }
+    t->net->init(A->Np, A->nb, info.nfaces, info.nfeat, info.nbr->data(), info.nfeat ? info.feats->data() : nullptr,
+                 0x5eed);
+  }
   switch (cfg.solver) {
     case BSGPU_SOLVER_SOFTPCG: {
       require(!mixed, "mixed precision is available for the FGMRES preconditioner", BSGPU_ERR_UNSUPPORTED);
@@ -1238,6 +1309,12 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
       } else {
         f->pc = build_level<double>(*t, A, A, 0, one);
       }
+      f->tree = t.get();
+      if (t->net && (cfg.learned & BSGPU_LEARNED_FGMRES)) {
+        f->pc2 = std::make_unique<LearnedPrecondT<double>>(*t->ctx, t->net.get());
+        f->pc2->trace = t->ctx->trace_id("LearnedStage");
+        f->stall = cfg.learned_stall > 0 ? cfg.learned_stall : 0.99;
+      }
       t->top = std::move(f);
       break;
     }
@@ -1246,6 +1323,53 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
   }
   BSGPU_CUDA(cudaStreamSynchronize(t->ctx->st));
   return t.release();
+}
+
+}  // namespace bsgpu
+
+namespace bsgpu {
+
+double train_learned(Tree& t, int n_rhs, int steps, double lr, uint64_t seed) {
+  require(t.net != nullptr, "the solver was created without the learned stage (cfg.learned = 0)");
+  require(n_rhs >= 1 && steps >= 1 && lr > 0, "n_rhs, steps and lr must be positive");
+  Ctx& c = *t.ctx;
+  const int64_t N = t.A->N;
+  // 1. training residuals generated by the solver itself: Arnoldi vectors of solves with random right-hand sides
+  std::vector<DBuf<double>> pool;
+  const bool was_on = t.learned_on;
+  t.learned_on = false;
+  t.collect = &pool;
+  t.collect_cap = (size_t)n_rhs * 12;
+  DBuf<double> b(std::max<int64_t>(N, 1)), x(std::max<int64_t>(N, 1));
+  for (int k = 0; k < n_rhs; ++k) {
+    fill_random(b.p, N, seed + 7919ull * k, c.st);
+    fill(0.0, x.p, N, c.st);
+    const size_t before = pool.size();
+    t.collect_cap = before + 12;
+    t.top->solve(c, x.p, b.p, true);
+    (void)before;
+  }
+  t.collect = nullptr;
+  require(!pool.empty(), "no training residuals were generated");
+  // 2. Adam on the energy-norm loss
+  DBuf<double> z(N), Az(N), g(N);
+  double* scal = c.scal(8);
+  double loss_acc = 0.0;
+  int loss_n = 0;
+  for (int s = 0; s < steps; ++s) {
+    learned_train_step(*t.net, *t.A, pool[s % pool.size()].p, z.p, Az.p, g.p, c.red, scal, lr, c.st);
+    if (s >= steps - 8) {
+      c.fetch(scal, 5);
+      const double* h = c.hscal + (scal - c.dscal.p);
+      loss_acc += (h[3] - 2.0 * h[4]) / h[2];
+      ++loss_n;
+    }
+  }
+  BSGPU_CUDA(cudaStreamSynchronize(c.st));
+  t.net->trained = true;
+  t.learned_on = true;
+  (void)was_on;
+  return loss_n ? loss_acc / loss_n : 0.0;
 }
 
 }  // namespace bsgpu

@@ -9,6 +9,7 @@
 #include "amg.cuh"
 #include "blas1.cuh"
 #include "blockops.cuh"
+#include "learned.cuh"
 #include "matrix.cuh"
 
 namespace bsgpu {
@@ -85,6 +86,11 @@ struct OperatorInfo {
   const Matrix* top = nullptr;
   const double* L = nullptr;  // device, per block row I x I row-major; nullptr for Eye
   const std::vector<HostBsr>* hprol = nullptr;
+  // cell graph for the learned stage: face neighbours per cell (-1 = none) and optional per-cell features
+  int nfaces = 0;
+  const std::vector<int32_t>* nbr = nullptr;
+  int nfeat = 0;
+  const std::vector<float>* feats = nullptr;
 };
 
 // Builds the solver tree for `cfg` on the (transformed) operator A (FP64).  For BSGPU_PRECISION_MIXED the
@@ -99,7 +105,16 @@ struct Tree {
   const Matrix* A = nullptr;
   bsgpu_solver_config cfg{};
   OperatorInfo info;
+  std::unique_ptr<LearnedNet> net;  // learned preconditioner stage (cfg.learned != 0)
+  bool learned_on = false;          // switched on once trained
+  // hooks used while generating training data: the outer FGMRES copies its Arnoldi vectors here
+  std::vector<DBuf<double>>* collect = nullptr;
+  size_t collect_cap = 0;
+  int learned_stalls = 0;           // solves in which the learned stage stalled and was switched off
 };
 Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info);
+// Generates training residuals with the solver itself (FGMRES Arnoldi vectors of solves with seeded random
+// right-hand sides, learned stage off) and trains the learned stage; returns the final mean loss.
+double train_learned(Tree& t, int n_rhs, int steps, double lr, uint64_t seed);
 
 }  // namespace bsgpu

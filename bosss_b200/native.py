@@ -18,6 +18,7 @@ TERM_DEFAULT, TERM_RELATIVE = 0, 1
 COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS = 0, 1
+LEARNED_OFF, LEARNED_FGMRES, LEARNED_PRESMOOTH, LEARNED_BOTH = 0, 1, 2, 3
 
 # every symbol the header declares (checked by the CPU test-suite)
 EXPORTS = [
@@ -27,7 +28,8 @@ EXPORTS = [
     "bsgpu_matrix_spmv_device_f32",
     "bsgpu_matrix_restrict",
     "bsgpu_mgop_create", "bsgpu_mgop_destroy", "bsgpu_mgop_get_operator", "bsgpu_mgop_add_h_level",
-    "bsgpu_mgop_read_left_cob",
+    "bsgpu_mgop_set_cell_neighbours", "bsgpu_mgop_set_cell_features", "bsgpu_mgop_read_left_cob",
+    "bsgpu_solver_train_learned",
     "bsgpu_solver_config_default", "bsgpu_solver_create", "bsgpu_solver_destroy", "bsgpu_solver_solve",
     "bsgpu_solver_solve_device", "bsgpu_solver_get_history", "bsgpu_solver_set_tracing", "bsgpu_solver_get_trace",
 ]
@@ -41,7 +43,8 @@ class SolverConfig(C.Structure):
                 ("coarse_max_iter", C.c_int32), ("sub_max_iter", C.c_int32), ("sub_reduction", C.c_double),
                 ("precision", C.c_int32), ("h_levels", C.c_int32), ("h_sweeps", C.c_int32), ("h_cycle", C.c_int32),
                 ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
-                ("reserved", C.c_int32 * 10)]
+                ("learned", C.c_int32), ("learned_hidden", C.c_int32), ("learned_stall", C.c_double),
+                ("reserved", C.c_int32 * 6)]
 
 
 class SolveStats(C.Structure):
@@ -93,6 +96,9 @@ def lib() -> C.CDLL:
             "bsgpu_mgop_get_operator": [vp, vp],
             "bsgpu_mgop_read_left_cob": [vp, vp],
             "bsgpu_mgop_add_h_level": [vp, i32, i64, i64, vp, vp, vp],
+            "bsgpu_mgop_set_cell_neighbours": [vp, i32, vp],
+            "bsgpu_mgop_set_cell_features": [vp, i32, vp],
+            "bsgpu_solver_train_learned": [vp, i32, i32, dbl, C.c_uint64, vp],
             "bsgpu_solver_config_default": [vp],
             "bsgpu_solver_create": [vp, vp, vp],
             "bsgpu_solver_destroy": [vp],

@@ -153,6 +153,17 @@ class MultigridOperator:
         for P in h_levels:
             self.AddHLevel(P)
 
+    def SetCellGraph(self, neighbours, features=None):
+        """Face neighbours per cell ([cells, faces], -1 = none) and optional per-cell features for the learned
+        stage."""
+        nb = np.ascontiguousarray(neighbours, np.int32)
+        nat.check(nat.lib().bsgpu_mgop_set_cell_neighbours(self._h, int(nb.shape[1]), nat.ptr(nb)))
+        if features is not None:
+            ft = np.ascontiguousarray(features, np.float32)
+            if ft.ndim == 1:
+                ft = ft[:, None]
+            nat.check(nat.lib().bsgpu_mgop_set_cell_features(self._h, int(ft.shape[1]), nat.ptr(ft)))
+
     def AddHLevel(self, P):
         rp = np.ascontiguousarray(P.row_ptr, np.int64)
         ci = np.ascontiguousarray(P.col_idx, np.int32)
@@ -274,6 +285,9 @@ class FGMRESConfig(IterativeSolverConfig):
     MaxKrylovDim: int = 30
     Preconditioners: List[PmgConfig] = field(default_factory=lambda: [PmgConfig()])
     MixedPrecision: bool = False
+    Learned: str = "off"            # "off" | "fgmres" | "presmooth" | "both"; needs MultigridOperator.SetCellGraph
+    LearnedHidden: int = 64
+    LearnedStall: float = 0.99
 
     def _config(self):
         if len(self.Preconditioners) != 1:
@@ -283,6 +297,13 @@ class FGMRESConfig(IterativeSolverConfig):
         c.max_krylov = self.MaxKrylovDim
         self.Preconditioners[0]._fill(c)
         c.precision = nat.PRECISION_MIXED if self.MixedPrecision else nat.PRECISION_FP64
+        modes = {"off": nat.LEARNED_OFF, "fgmres": nat.LEARNED_FGMRES, "presmooth": nat.LEARNED_PRESMOOTH,
+                 "both": nat.LEARNED_BOTH}
+        if self.Learned not in modes:
+            raise ValueError(f"Learned must be one of {sorted(modes)}")
+        c.learned = modes[self.Learned]
+        c.learned_hidden = self.LearnedHidden
+        c.learned_stall = self.LearnedStall
         return c
 
 
@@ -367,6 +388,13 @@ class GpuSolver:
         out = np.zeros(max(n.value, 1))
         nat.check(nat.lib().bsgpu_solver_get_history(self._h, nat.ptr(out), n.value, C.byref(n)))
         return out[:n.value]
+
+    def TrainLearned(self, n_rhs: int = 2, steps: int = 200, lr: float = 1e-3, seed: int = 0) -> float:
+        """Trains the learned stage on residuals this solver generates; returns the final mean energy loss."""
+        loss = C.c_double()
+        nat.check(nat.lib().bsgpu_solver_train_learned(self._h, int(n_rhs), int(steps), float(lr), int(seed),
+                                                       C.byref(loss)))
+        return loss.value
 
     def SetTracing(self, on: bool = True):
         nat.check(nat.lib().bsgpu_solver_set_tracing(self._h, 1 if on else 0))

@@ -110,6 +110,11 @@ BSGPU_API int bsgpu_mgop_get_operator(bsgpu_mgop_t op, bsgpu_matrix_t* Aop);
  * (MultigridOperator.cs:774,815; AggregationGridBasis.cs); used by BSGPU_COARSE_HMG. */
 BSGPU_API int bsgpu_mgop_add_h_level(bsgpu_mgop_t op, int32_t Np, int64_t nb_fine, int64_t nb_coarse,
                                      const int64_t* row_ptr, const int32_t* col_idx, const double* values);
+/* Cell graph for the learned stage: nb x nfaces face-neighbour indices (-1 where a face has no neighbour), and
+ * optional per-cell input features (nb x nfeat floats, e.g. log of the diffusivity of the cell and its
+ * neighbours).  Host pointers; copied. */
+BSGPU_API int bsgpu_mgop_set_cell_neighbours(bsgpu_mgop_t op, int32_t nfaces, const int32_t* nbr);
+BSGPU_API int bsgpu_mgop_set_cell_features(bsgpu_mgop_t op, int32_t nfeat, const float* feats);
 /* Per-block L factors, row-major, concatenated in block order (host buffer). */
 BSGPU_API int bsgpu_mgop_read_left_cob(bsgpu_mgop_t op, double* L);
 
@@ -131,6 +136,11 @@ enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in 
 /* post-smoother of the OrthoMG levels: BlockJacobi (BlockJacobi.cs:35; NoOfIterations = bj_iters), or symmetric
  * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20) */
 enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1 };
+/* learned preconditioner stage (no counterpart in the reference): a one-hop message-passing MLP over the cell
+ * graph, BF16 weights, FP32 accumulation.  FGMRES: an extra FlexGMRES preconditioner used in turn with the
+ * p-multigrid V-cycle (FlexGMRES.cs:196-199 round-robin); PRESMOOTH: pre-smoother of the finest OrthoMG level
+ * (OrthonormalizationMultigrid.cs:899); plain p-multigrid takes over when the stage stalls. */
+enum { BSGPU_LEARNED_OFF = 0, BSGPU_LEARNED_FGMRES = 1, BSGPU_LEARNED_PRESMOOTH = 2, BSGPU_LEARNED_BOTH = 3 };
 
 typedef struct {
   int32_t solver;           /* BSGPU_SOLVER_*                                                   */
@@ -156,7 +166,11 @@ typedef struct {
   int32_t dense_limit;      /* levels with at most this many unknowns are solved densely        */
   int32_t smoother;         /* BSGPU_SMOOTHER_* on the p-levels                                 */
   int32_t h_smoother;       /* BSGPU_SMOOTHER_* on the h-levels (aggregation / h-multigrid)     */
-  int32_t reserved[10];
+  int32_t learned;          /* BSGPU_LEARNED_* (needs cell neighbours on the operator)          */
+  int32_t learned_hidden;   /* hidden width of the learned stage (multiple of 16, default 64)   */
+  double learned_stall;     /* a learned step reducing the residual by less than this factor
+                               switches the stage off for the rest of the solve (default 0.99)  */
+  int32_t reserved[6];
 } bsgpu_solver_config;
 
 typedef struct {
@@ -182,6 +196,11 @@ BSGPU_API int bsgpu_solver_get_history(bsgpu_solver_t s, double* hist, int32_t c
  * inclusive seconds and iterations (the stream is synchronised at block boundaries, so leave it off when timing
  * the whole solve).  Also switched on by the environment variable BSGPU_TRACE=1.  get_trace writes a JSON array. */
 BSGPU_API int bsgpu_solver_set_tracing(bsgpu_solver_t s, int32_t on);
+/* Trains the learned stage (cfg.learned != 0) on residuals the solver itself generates: the Arnoldi vectors of
+ * n_rhs solves with seeded random right-hand sides (learned stage off), then `steps` Adam steps at learning rate
+ * lr on the energy-norm loss.  Switches the stage on.  loss (may be NULL): final mean loss. */
+BSGPU_API int bsgpu_solver_train_learned(bsgpu_solver_t s, int32_t n_rhs, int32_t steps, double lr, uint64_t seed,
+                                         double* loss);
 BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len);
 
 #ifdef __cplusplus

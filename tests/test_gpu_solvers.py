@@ -238,3 +238,29 @@ def test_block_gauss_seidel_smoother(cuda, mixed):
     xd = _direct(s)
     assert slv.Converged
     assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("mode", ["fgmres", "presmooth", "both"])
+def test_learned_stage_trains_and_solves(cuda, mode):
+    """Learned preconditioner stage: trains on solver-generated residuals (energy loss below that of a zero
+    correction) and FGMRES still converges to the direct solution with the stage in place."""
+    s = A.poisson_3d(8, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    op.SetCellGraph(s.grid.face_neighbours())
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseTolerance=1e-1, CoarseMaxIterations=60)
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
+                       MixedPrecision=True, Learned=mode).CreateInstance(op)
+    loss = slv.TrainLearned(n_rhs=1, steps=60, lr=2e-3, seed=3)
+    assert loss < 0.0
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+def test_learned_stage_needs_cell_graph(cuda):
+    s = A.poisson_3d(4, 2)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    with pytest.raises(ValueError):
+        FGMRESConfig(Preconditioners=[PmgConfig(DegreeHierarchy=(10, 4))], Learned="fgmres").CreateInstance(op)
