@@ -230,6 +230,129 @@ __global__ void trsv_lt_kernel(const int32_t* __restrict__ len, const int64_t* _
   }
 }
 
+// Restricted additive Schwarz factors with one block per cell: the block of cell K is K plus the cells its block
+// row couples to (face neighbours, i.e. overlap 1).  The dense block matrix is assembled in shared memory,
+// inverted by Gauss-Jordan with partial pivoting in FP64, and the rows of cell K are written into M, which has
+// A's block structure: M_{K,L} = [P_K^-1]_{K,L}.  One CTA per cell; block sizes may differ between cells.
+template <typename TO>
+__global__ void schwarz_factor_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                      const int32_t* __restrict__ len, const int64_t* __restrict__ boff,
+                                      const double* __restrict__ vals, int V, const int64_t* __restrict__ boffM,
+                                      int VM, TO* __restrict__ M, int maxp, int* __restrict__ err, int64_t nb) {
+  extern __shared__ double sm[];
+  __shared__ int offs[33];
+  __shared__ int piv;
+  __shared__ int bad;
+  for (int64_t K = blockIdx.x; K < nb; K += gridDim.x) {
+    const int64_t k0 = rp[K], k1 = rp[K + 1];
+    const int nc = (int)(k1 - k0);
+    if (threadIdx.x == 0) {
+      bad = nc > 32;
+      int o = 0;
+      for (int a = 0; a < nc && a < 32; ++a) {
+        offs[a] = o;
+        o += len[ci[k0 + a]];
+      }
+      offs[nc < 32 ? nc : 32] = o;
+      if (o > maxp) bad = 1;
+    }
+    __syncthreads();
+    if (bad) {
+      if (threadIdx.x == 0) atomicCAS(err, 0, (int)(K + 1 < 0x7fffffff ? K + 1 : 0x7fffffff));
+      __syncthreads();
+      continue;
+    }
+    const int n = offs[nc];
+    double* P = sm;                 // n x n
+    double* prow = sm + n * n;
+    double* pcol = prow + n;
+    int* perm = reinterpret_cast<int*>(pcol + n);
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) P[e] = 0.0;
+    __syncthreads();
+    // assemble: for every patch cell a, the blocks of its row whose column is a patch cell
+    for (int a = 0; a < nc; ++a) {
+      const int32_t ca = ci[k0 + a];
+      const int I = len[ca];
+      for (int64_t q = rp[ca]; q < rp[ca + 1]; ++q) {
+        const int32_t cb = ci[q];
+        int b = -1;
+        for (int t = 0; t < nc; ++t)
+          if (ci[k0 + t] == cb) b = t;
+        if (b < 0) continue;
+        const int J = len[cb];
+        for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+          const int r = e / J, c = e - r * J;
+          P[(offs[a] + r) * n + offs[b] + c] = vals[boff[q] + (int64_t)(c / V) * I * V + r * V + (c % V)];
+        }
+      }
+    }
+    __syncthreads();
+    // Gauss-Jordan inversion with partial pivoting
+    for (int p = 0; p < n; ++p) {
+      if (threadIdx.x == 0) {
+        int best = p;
+        double mx = fabs(P[p * n + p]);
+        for (int r = p + 1; r < n; ++r)
+          if (fabs(P[r * n + p]) > mx) { mx = fabs(P[r * n + p]); best = r; }
+        piv = best;
+        perm[p] = best;
+        if (!(mx > 0.0) || !isfinite(mx)) { bad = 1; atomicCAS(err, 0, (int)(K + 1 < 0x7fffffff ? K + 1 : 0x7fffffff)); }
+      }
+      __syncthreads();
+      if (bad) break;
+      if (piv != p)
+        for (int c = threadIdx.x; c < n; c += blockDim.x) {
+          const double t = P[p * n + c];
+          P[p * n + c] = P[piv * n + c];
+          P[piv * n + c] = t;
+        }
+      __syncthreads();
+      const double inv = 1.0 / P[p * n + p];
+      for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        prow[q] = (q == p) ? inv : P[p * n + q] * inv;
+        pcol[q] = P[q * n + p];
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+        const int r = e / n, c = e - r * n;
+        if (r == p)
+          P[e] = prow[c];
+        else if (c == p)
+          P[e] = -pcol[r] * prow[p];
+        else
+          P[e] -= pcol[r] * prow[c];
+      }
+      __syncthreads();
+    }
+    if (!bad) {
+      for (int p = n - 1; p >= 0; --p) {
+        const int q = perm[p];
+        if (q != p)
+          for (int r = threadIdx.x; r < n; r += blockDim.x) {
+            const double t = P[r * n + p];
+            P[r * n + p] = P[r * n + q];
+            P[r * n + q] = t;
+          }
+        __syncthreads();
+      }
+      // rows of the centre cell K -> block row K of M
+      int aK = 0;
+      for (int t = 0; t < nc; ++t)
+        if (ci[k0 + t] == K) aK = t;
+      const int I = len[K];
+      for (int b = 0; b < nc; ++b) {
+        const int J = len[ci[k0 + b]];
+        for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+          const int r = e / J, c = e - r * J;
+          M[boffM[k0 + b] + (int64_t)(c / VM) * I * VM + r * VM + (c % VM)] =
+              (TO)P[(offs[aK] + r) * n + offs[b] + c];
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
 DBuf<int32_t> blk_rows(const Matrix& A) {
   std::vector<int32_t> br(A.nnzb);
   for (int64_t i = 0; i < A.nb; ++i)
@@ -278,6 +401,34 @@ void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cuda
   if (smem > 48 * 1024) BSGPU_CUDA(cudaFuncSetAttribute(invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   invert_kernel<<<grid_for(A.nb), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, A.doff.p, D64, D32,
                                                   err, A.nb);
+  BSGPU_CHECK_LAUNCH();
+}
+
+void schwarz_factor(const Matrix& A, Matrix& M, int* err, cudaStream_t st) {
+  require(!A.single, "Schwarz factorisation needs the FP64 matrix");
+  if (A.nb == 0) return;
+  // largest patch: the block row with the most DOFs
+  int64_t maxp = 0;
+  for (int64_t i = 0; i < A.nb; ++i) {
+    int64_t s = 0;
+    for (int64_t k = A.h_rp[i]; k < A.h_rp[i + 1]; ++k) s += A.h_len[A.h_ci[k]];
+    maxp = std::max(maxp, s);
+    require(A.h_rp[i + 1] - A.h_rp[i] <= 32, "Schwarz: more than 32 coupled cells in a block row",
+            BSGPU_ERR_UNSUPPORTED);
+  }
+  const size_t smem = (size_t)(maxp * maxp + 2 * maxp) * 8 + (size_t)maxp * 4;
+  require(smem <= 220 * 1024, "Schwarz: patch of " + std::to_string(maxp) + " unknowns exceeds shared memory",
+          BSGPU_ERR_UNSUPPORTED);
+  const int grid = (int)std::min<int64_t>(A.nb, (int64_t)num_sms() * 8);
+  if (M.single) {
+    BSGPU_CUDA(cudaFuncSetAttribute(schwarz_factor_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    schwarz_factor_kernel<float><<<grid, 256, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, M.boff.p,
+                                                          M.V, M.v32.p, (int)maxp, err, A.nb);
+  } else {
+    BSGPU_CUDA(cudaFuncSetAttribute(schwarz_factor_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    schwarz_factor_kernel<double><<<grid, 256, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, M.boff.p,
+                                                           M.V, M.v64.p, (int)maxp, err, A.nb);
+  }
   BSGPU_CHECK_LAUNCH();
 }
 

@@ -12,6 +12,11 @@ void change_of_basis_apply(const Matrix& A, const double* L, Matrix& Aout, cudaS
 // Inverses of the diagonal blocks (BlockJacobi.cs:125-146 InvertInPlace), stored column-major per block at
 // diag_offsets(A); computed in FP64 and written as FP64 (D64) and/or FP32 (D32).
 void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cudaStream_t st);
+// Restricted additive Schwarz factors, one overlapping block per cell (the cell and the cells of its block
+// row): M (A's structure, FP64 or FP32 values) gets the centre-cell rows of each block inverse
+// (Schwarz.cs:623-840 block set-up; blocks here are cell patches with overlap 1).  One launch for all blocks,
+// whatever their sizes.
+void schwarz_factor(const Matrix& A, Matrix& M, int* err, cudaStream_t st);
 // y_i = L_i^{-T} x_i per block (initial-guess transform with a lower-triangular L, row-major).
 void block_trsv_lt(const Matrix& A, const double* L, const double* x, double* y, cudaStream_t st);
 

@@ -188,6 +188,37 @@ struct BlockGST : Solver<T> {
   }
 };
 
+// Additive Schwarz smoother (Schwarz.cs:56; Init :623-840, Solve :996-1147) in restricted form with one
+// overlapping block per cell (schwarz_factor in blockops.cu): x <- x + M (b - A x), M holding the centre rows of
+// the block inverses, stored in FP32 for the mixed-precision preconditioner.  bj_iters + 1 updates per call, as
+// for BlockJacobi.
+template <typename T>
+struct SchwarzT : Solver<T> {
+  const Matrix* A;
+  std::unique_ptr<Matrix> M;
+  DBuf<T> r;
+  int updates;
+  SchwarzT(Ctx& c, const Matrix* A64, const Matrix* AT, int iters) : A(AT), updates(iters + 1) {
+    M.reset(matrix_like(*A64, sizeof(T) == 4));
+    int* err = c.flag();
+    schwarz_factor(*A64, *M, err, c.st);
+    c.check_flag(err, "Schwarz: singular block");
+    r.alloc(std::max<int64_t>(A->N, 1));
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    for (int s = 0; s < updates; ++s) {
+      if (s == 0 && zero) {
+        spmv(*M, T(1), B, T(0), (const T*)nullptr, X, c.st);
+      } else {
+        spmv(*A, T(-1), X, T(1), B, r.p, c.st);
+        spmv(*M, T(1), r.p, T(1), X, X, c.st);
+      }
+    }
+    this->converged = true;
+  }
+};
+
 // ---------------------------------------------------------------------------------------------------------------
 // PCG with a block-diagonal preconditioner (SoftPCG.cs:113-194; also the coarsest-level solve).  The iteration
 // runs on device scalars; its kernels are predicated on a device flag that the convergence test clears, so the
@@ -1120,11 +1151,17 @@ template <typename T>
 std::unique_ptr<Solver<T>> make_smoother(Ctx& c, const Matrix* A64, const Matrix* AT, int kind,
                                          const bsgpu_solver_config& cfg, const std::string& name) {
   std::unique_ptr<Solver<T>> s;
-  if (kind == BSGPU_SMOOTHER_BLOCKGS)
+  const char* tag = ".BlockJacobi";
+  if (kind == BSGPU_SMOOTHER_BLOCKGS) {
     s = std::make_unique<BlockGST<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
-  else
+    tag = ".BlockGS";
+  } else if (kind == BSGPU_SMOOTHER_SCHWARZ) {
+    s = std::make_unique<SchwarzT<T>>(c, A64, AT, cfg.bj_iters);
+    tag = ".Schwarz";
+  } else {
     s = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
-  s->trace = c.trace_id(name + (kind == BSGPU_SMOOTHER_BLOCKGS ? ".BlockGS" : ".BlockJacobi"));
+  }
+  s->trace = c.trace_id(name + tag);
   return s;
 }
 
@@ -1289,7 +1326,8 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
       break;
     }
     case BSGPU_SOLVER_BLOCKJACOBI:
-      t->top = std::make_unique<BlockJacobiT<double>>(*t->ctx, A, A, cfg.bj_iters, cfg.bj_omega);
+      require(!mixed, "mixed precision is available for the FGMRES preconditioner", BSGPU_ERR_UNSUPPORTED);
+      t->top = make_smoother<double>(*t->ctx, A, A, cfg.smoother, cfg, "");
       break;
     case BSGPU_SOLVER_ORTHOMG:
       require(!mixed, "mixed precision is available for the FGMRES preconditioner", BSGPU_ERR_UNSUPPORTED);

@@ -17,7 +17,7 @@ SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI = 0, 1, 2,
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS = 0, 1
+SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS, SMOOTHER_SCHWARZ = 0, 1, 2
 LEARNED_OFF, LEARNED_FGMRES, LEARNED_PRESMOOTH, LEARNED_BOTH = 0, 1, 2, 3
 
 # every symbol the header declares (checked by the CPU test-suite)

@@ -262,7 +262,8 @@ class PmgConfig(IterativeSolverConfig):
         c.h_sweeps = self.HSweeps
         c.h_cycle = self.HCycle
         c.dense_limit = self.DenseLimit
-        sm = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "blockgs": nat.SMOOTHER_BLOCKGS}
+        sm = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "blockgs": nat.SMOOTHER_BLOCKGS,
+              "schwarz": nat.SMOOTHER_SCHWARZ}
         if self.Smoother not in sm or self.HSmoother not in sm:
             raise ValueError(f"Smoother / HSmoother must be one of {sorted(sm)}")
         c.smoother = sm[self.Smoother]
@@ -331,6 +332,30 @@ class BlockJacobiConfig:
         c.solver = nat.SOLVER_BLOCKJACOBI
         c.bj_iters = self.NoOfIterations
         c.bj_omega = self.omega
+        return GpuSolver(op, c)
+
+
+@dataclass
+class SchwarzConfig:
+    """Schwarz.Config (Schwarz.cs:424) as a stand-alone solver: FixedNoOfIterations (Schwarz.cs:979) updates of
+    restricted additive Schwarz with one block per cell plus its face neighbours (``Overlap`` = 1).
+
+    The reference's METIS blocking with ``EnableOverlapScaling`` is replaced by per-cell blocks whose correction is
+    written to the centre cell only (the restricted form), which needs no scaling of the overlap.
+    """
+    FixedNoOfIterations: int = 1
+    Overlap: int = 1
+
+    def CreateInstance(self, op: MultigridOperator) -> "GpuSolver":
+        if self.Overlap != 1:
+            raise NotImplementedError("Schwarz blocks are one cell plus its face neighbours (Overlap = 1)")
+        if self.FixedNoOfIterations < 1:
+            raise ValueError("FixedNoOfIterations must be at least 1")
+        c = nat.SolverConfig()
+        nat.check(nat.lib().bsgpu_solver_config_default(C.byref(c)))
+        c.solver = nat.SOLVER_BLOCKJACOBI
+        c.smoother = nat.SMOOTHER_SCHWARZ
+        c.bj_iters = self.FixedNoOfIterations - 1
         return GpuSolver(op, c)
 
 

@@ -123,7 +123,7 @@ enum {
   BSGPU_SOLVER_SOFTPCG = 0,     /* SoftPCG.cs:113 with a block-Jacobi preconditioner (or none)              */
   BSGPU_SOLVER_FGMRES_PMG = 1,  /* FlexGMRES.cs:144 (Saad FGMRES(m)) preconditioned by one p-MG V-cycle     */
   BSGPU_SOLVER_ORTHOMG = 2,     /* PmgConfig.cs:80 OrthonormalizationMultigrid p-multigrid as the solver    */
-  BSGPU_SOLVER_BLOCKJACOBI = 3  /* BlockJacobi.cs:35 as a standalone smoother                               */
+  BSGPU_SOLVER_BLOCKJACOBI = 3  /* the smoother cfg.smoother selects (BlockJacobi.cs:35, Schwarz.cs:56) alone */
 };
 enum { BSGPU_TERM_DEFAULT = 0 /* R < R0*tol + tol */, BSGPU_TERM_RELATIVE = 1 /* R < R0*tol */ };
 /* coarsest-level solver: dense inverse (p = 0, <= 4096 unknowns), block-Jacobi PCG, or PCG preconditioned by a
@@ -133,9 +133,11 @@ enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1, BSGPU_COARSE_AMG = 2,
                                OrthoMG to coarse_tol with h_sweeps block-Jacobi sweeps, h_cycle iterations on the
                                coarser h-levels, dense below dense_limit */ };
 enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in FP32, outer FP64 */ };
-/* post-smoother of the OrthoMG levels: BlockJacobi (BlockJacobi.cs:35; NoOfIterations = bj_iters), or symmetric
- * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20) */
-enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1 };
+/* post-smoother of the OrthoMG levels: BlockJacobi (BlockJacobi.cs:35; NoOfIterations = bj_iters), symmetric
+ * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20), or
+ * restricted additive Schwarz with one overlapping block per cell (Schwarz.cs:56; bj_iters + 1 updates; blocks
+ * of up to ~160 unknowns, uneven sizes allowed), factors in FP32 for the mixed-precision preconditioner */
+enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1, BSGPU_SMOOTHER_SCHWARZ = 2 };
 /* learned preconditioner stage (no counterpart in the reference): a one-hop message-passing MLP over the cell
  * graph, BF16 weights, FP32 accumulation.  FGMRES: an extra FlexGMRES preconditioner used in turn with the
  * p-multigrid V-cycle (FlexGMRES.cs:196-199 round-robin); PRESMOOTH: pre-smoother of the finest OrthoMG level

@@ -818,6 +818,51 @@ int or_restrict(const or_bsr* m, int keep, double* values_out, int64_t* map_out)
   }
 }
 
+// Schwarz block set-up restated for blocks = one cell plus the cells of its block row (overlap 1), restricted
+// form: the rows of the centre cell of each block inverse (Schwarz.cs:623-840 extracts each block's sub-matrix
+// and factors it with LAPACK; here the sub-matrix is inverted with InvertInPlace).  values_out has A's layout.
+int or_schwarz_rows(const or_bsr* m, double* values_out) {
+  try {
+    Mat A;
+    load_mat(A, m);
+    int err = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : err)
+    for (int64_t K = 0; K < A.nb; ++K) {
+      std::vector<int32_t> cells(A.ci.begin() + A.rp[K], A.ci.begin() + A.rp[K + 1]);
+      std::vector<int> off(cells.size() + 1, 0);
+      for (size_t a = 0; a < cells.size(); ++a) off[a + 1] = off[a] + A.len[cells[a]];
+      const int n = off.back();
+      std::vector<double> P((size_t)n * n, 0.0);
+      for (size_t a = 0; a < cells.size(); ++a) {
+        const int32_t ca = cells[a];
+        for (int64_t q = A.rp[ca]; q < A.rp[ca + 1]; ++q) {
+          auto it = std::find(cells.begin(), cells.end(), A.ci[q]);
+          if (it == cells.end()) continue;
+          const size_t b = it - cells.begin();
+          const int I = A.len[ca], J = A.len[A.ci[q]];
+          const double* blk = A.blk(q);
+          for (int r = 0; r < I; ++r)
+            for (int c = 0; c < J; ++c) P[(size_t)(off[a] + r) * n + off[b] + c] = blk[r * J + c];
+        }
+      }
+      err |= invert(n, P.data());
+      const size_t aK = std::find(cells.begin(), cells.end(), (int32_t)K) - cells.begin();
+      const int I = A.len[K];
+      for (size_t b = 0; b < cells.size(); ++b) {
+        const int J = A.len[cells[b]];
+        double* o = values_out + A.vp[A.rp[K] + b];
+        for (int r = 0; r < I; ++r)
+          for (int c = 0; c < J; ++c) o[r * J + c] = P[(size_t)(off[aK] + r) * n + off[b] + c];
+      }
+    }
+    if (err) { g_err = "Schwarz: singular block"; return OR_ERR_ARITHMETIC; }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return OR_ERR_ARGUMENT;
+  }
+}
+
 int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const double* b) {
   try {
     Mat A;

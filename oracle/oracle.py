@@ -148,6 +148,13 @@ def restrict(A: Bsr, keep: int):
     return out, mp
 
 
+def schwarz_rows(A: Bsr) -> np.ndarray:
+    """Centre-cell rows of the inverse of every cell-plus-neighbours block, in A's block layout."""
+    out = np.empty_like(A.values)
+    _check(lib().or_schwarz_rows(C.byref(A._c), out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
 def blockjacobi(A: Bsr, x: np.ndarray, b: np.ndarray, iters: int = 1, omega: float = 1.0) -> np.ndarray:
     x = np.ascontiguousarray(x, np.float64).copy()
     b = np.ascontiguousarray(b, np.float64)
