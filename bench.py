@@ -50,6 +50,12 @@ def parse():
     ap.add_argument("--spmv-only", action="store_true",
                     help="only the stand-alone SpMV timing (profiling runs; prints a short JSON line)")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--workload", default="poisson64", choices=["poisson64", "xdg48", "varcoef96", "xdgbatch"],
+                    help="poisson64: the default solve above; xdg48: two-species sphere, 48^3 p=2; varcoef96: "
+                         "k = exp(GRF) diffusion, 96^3 p=2; xdgbatch: 256 independent sphere problems")
+    ap.add_argument("--batch", type=int, default=256, help="xdgbatch: number of problems")
+    ap.add_argument("--concurrency", type=int, default=16, help="xdgbatch: problems solved at once")
+    ap.add_argument("--learned", default="off", help="varcoef96/xdgbatch: learned stage mode")
     return ap.parse_args()
 
 
@@ -115,30 +121,18 @@ class ClockSampler:
 
 
 def dist_init():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    return ws, rank, local
+    from bosss_b200 import replicas
+    return replicas.init("nccl")
 
 
 def max_over_ranks(v: float, ws: int) -> float:
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from bosss_b200 import replicas
+    return replicas.max_over_ranks(v, ws)
 
 
 def barrier(ws: int):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from bosss_b200 import replicas
+    replicas.barrier(ws)
 
 
 # ----------------------------------------------------------------------------------------------------------------
@@ -428,16 +422,267 @@ def _traffic_per_launch():
     return None
 
 
+# ----------------------------------------------------------------------------------------------------------------
+# The other workloads: one XDG system, the variable-coefficient system, the batch of XDG systems
+# ----------------------------------------------------------------------------------------------------------------
+XDG48 = ("XDG sphere Poisson 48^3 hex, p=2 (Np=10, 20 in cut cells), mu 1:1000, FlexGMRES(30) + 3-level p-MG "
+         "(p=2->1->0)")
+VARCOEF96 = ("SIP diffusion k=exp(g), g a squared-exponential GRF (l=0.1, var 1), 96^3 hex, p=2 (Np=10, 8.85M DOF), "
+             "FlexGMRES(30) + 3-level p-MG (p=2->1->0)")
+XDGBATCH = ("independent XDG sphere problems, edge in {16,24,32,40,48}, p=2, radius U[0.15,0.35], jump in "
+            "{10,100,1000}, FlexGMRES(30) + 3-level p-MG (p=2->1->0)")
+# p-multigrid settings of these workloads: FP32 Schwarz smoothing (4 post-sweeps) for the fast path, the plain
+# FP64 path as in the default workload (block Jacobi, 10 post-sweeps)
+PMG_SCHWARZ = dict(NoOfPostSmootherSweeps=4, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.1,
+                   CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, Smoother="schwarz")
+PMG_BJ = dict(SOLVER_PARAMS, Smoother="blockjacobi")
+
+
+def spmv_bytes_blocks(s) -> int:
+    """Algorithmic bytes of one y = A*x for blocks of any size (nspc*Np rows per block row)."""
+    lens = s.Np * (np.ones(s.nb, np.int64) if getattr(s, "nspc", None) is None else s.nspc.astype(np.int64))
+    rows = np.repeat(np.arange(s.nb), np.diff(s.row_ptr))
+    blk = int((lens[rows] * lens[s.col_idx]).sum())
+    return blk * 8 + len(s.col_idx) * 4 + (s.nb + 1) * 8 + 2 * int(lens.sum()) * 8
+
+
+def _fgmres(op, pmg: dict, mixed: bool, learned: str = "off"):
+    from bosss_b200.solvers import FGMRESConfig, PmgConfig
+    return FGMRESConfig(ConvergenceCriterion=TOL, termination="relative", MaxKrylovDim=30, MaxSolverIterations=300,
+                        Preconditioners=[PmgConfig(DegreeHierarchy=(10, 4, 1), **pmg)], MixedPrecision=mixed,
+                        Learned=learned).CreateInstance(op)
+
+
+def _time_solve(slv, X, B, stream, reps=1):
+    import torch
+    out = []
+    for _ in range(reps):
+        X.zero_()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        slv.Solve(X, B)
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b) * 1e-3)
+    return out
+
+
+def run_single_system(args, s, workload, prepare=None):
+    """One system: FP64 SpMV alone, the plain FP64 solve, the fast solve (K timed steps), e2e with host buffers."""
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from bosss_b200 import native as nat
+    from bosss_b200.solvers import BlockMsrMatrix, MultigridOperator
+    nat.check(nat.lib().bsgpu_set_device(local))
+    M = BlockMsrMatrix.from_system(s)
+    t0 = time.perf_counter()
+    op = MultigridOperator(M)
+    if prepare is not None:
+        prepare(op)
+    torch.cuda.synchronize()
+    t_cob = time.perf_counter() - t0
+    stream = torch.cuda.current_stream()
+    Aop = op.OperatorMatrix
+    x = torch.randn(s.N, dtype=torch.float64, device=dev)
+    y = torch.zeros_like(x)
+    for _ in range(5):
+        Aop.SpMV(1.0, x, 0.0, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.spmv_repeats):
+        Aop.SpMV(1.0, x, 0.0, y)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = e0.elapsed_time(e1) / args.spmv_repeats
+    nbytes = spmv_bytes_blocks(s)
+    spmv_gbs = nbytes / (spmv_ms * 1e-3) / 1e9
+    del x, y
+
+    B = torch.from_numpy(s.rhs).to(dev)
+    X = torch.zeros_like(B)
+    variants = {"plain_fp64": (PMG_BJ, False, "off"), "fp64_schwarz": (PMG_SCHWARZ, False, "off"),
+                "fast": (PMG_SCHWARZ, True, args.learned)}
+    res = {}
+    x_plain = None
+    fast = None
+    train_s = None
+    for name, (pmg, mixed, learned) in variants.items():
+        t0 = time.perf_counter()
+        slv = _fgmres(op, pmg, mixed, learned)
+        torch.cuda.synchronize()
+        setup = time.perf_counter() - t0
+        if learned != "off":
+            t0 = time.perf_counter()
+            slv.TrainLearned(n_rhs=4, steps=200, lr=2e-3, seed=1)
+            torch.cuda.synchronize()
+            train_s = time.perf_counter() - t0
+        if name == "fast":
+            fast = slv
+            fast_setup = setup
+            continue
+        _time_solve(slv, X, B, stream)          # warm-up
+        t = _time_solve(slv, X, B, stream, reps=2)
+        res[name] = {"value": min(t), "unit": "s", "iters": slv.ThisLevelIterations, "converged": slv.Converged,
+                     "final_relres": _true_relres(Aop, op, X, B, s), "setup_s": setup}
+        if name == "plain_fp64":
+            x_plain = X.clone()
+        slv.Dispose()
+
+    for _ in range(args.warmup):
+        _time_solve(fast, X, B, stream)
+    barrier(ws)
+    launches0 = nat.launch_count()
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            X.zero_()
+            fast.Solve(X, B)
+        b.record(stream)
+        torch.cuda.synchronize()
+    launches = nat.launch_count() - launches0
+    t_fast = max_over_ranks(a.elapsed_time(b) * 1e-3 / args.steps, ws)
+    fast_res = _true_relres(Aop, op, X, B, s)
+    sol_diff = (torch.linalg.norm(X - x_plain) / torch.linalg.norm(x_plain)).item()
+    bh = torch.from_numpy(s.rhs).pin_memory()
+    xh = torch.zeros(s.N, dtype=torch.float64).pin_memory()
+    bn, xn = bh.numpy(), xh.numpy()
+    e2e = []
+    for i in range(1 + min(args.steps, 2)):
+        xn[:] = 0.0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fast.Solve(xn, bn)
+        if i > 0:
+            e2e.append(time.perf_counter() - t0)
+    e2e_t = max_over_ranks(sum(e2e) / len(e2e), ws)
+    clocks = clk.summary()
+    if rank != 0:
+        return
+    peaks = _peaks()
+    line = {
+        "metric": METRIC, "value": t_fast, "unit": "s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_fast * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 (outer) / f32 (preconditioner)", "data": "synthetic (seeded, assembled in-repo)",
+        "config": {"workload": workload, "dof": s.N, "blocks": len(s.col_idx), "tol": TOL,
+                   "l2": f"inputs larger than L2 ({nbytes / 1e9:.2f} GB per SpMV)", "parallelism": f"replicas x{ws}",
+                   "fast": "FP32 Schwarz p-MG inside FP64 FlexGMRES" + ("" if args.learned == "off" else
+                                                                        f" + learned stage ({args.learned})"),
+                   "plain": "FP64 block-Jacobi p-MG inside FP64 FlexGMRES"},
+        "iters": fast.ThisLevelIterations, "final_relres": fast_res, "fast_setup_s": fast_setup,
+        "learned_train_s": train_s,
+        **res,
+        "speedup_vs_plain_fp64": res["plain_fp64"]["value"] / t_fast,
+        "speedup_vs_fp64_schwarz": res["fp64_schwarz"]["value"] / t_fast,
+        "rel_diff_vs_plain_fp64_solution": sol_diff,
+        "spmv": {"gbs": spmv_gbs, "ms": spmv_ms, "bytes": nbytes, "repeats": args.spmv_repeats},
+        "setup": {"change_of_basis_s": t_cob},
+        "roofline": {"bound": "hbm", "achieved": spmv_gbs, "peak": peaks[0], "unit": "GB/s",
+                     "frac": spmv_gbs / peaks[0], "traffic": None, "kernel": "FP64 block SpMV on this system",
+                     "peak_source": peaks[1]},
+        "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": 2 * s.N * 8, "d2h_bytes_per_step": s.N * 8},
+        "gpu_launches": launches, "clocks": clocks,
+        "cpu_baseline": None,
+    }
+    fast.Dispose()
+    print(json.dumps(line), flush=True)
+
+
+def _gen_xdg(spec):
+    from bosss_b200 import xdg
+    return xdg.xdg_sphere(**spec)
+
+
+def _bounded_imap(pool, fn, items, ahead):
+    """pool.imap with at most `ahead` results outstanding (bounds host memory)."""
+    pending = []
+    items = list(items)
+    i = 0
+    while i < len(items) or pending:
+        while i < len(items) and len(pending) < ahead:
+            pending.append(pool.apply_async(fn, (items[i],)))
+            i += 1
+        yield pending.pop(0).get()
+
+
+def run_xdg_batch(args):
+    """Batch of independent XDG problems: generated on the host cores (a spawn pool started before any CUDA call),
+    set up and solved in waves of `concurrency` problems, every problem with the fast and the plain FP64 path."""
+    import multiprocessing as mp
+    from bosss_b200 import xdg
+    ws, rank, local = (int(os.environ.get(k, d)) for k, d in (("WORLD_SIZE", "1"), ("RANK", "0"),
+                                                              ("LOCAL_RANK", "0")))
+    specs = xdg.batch_specs(args.batch, seed=args.seed)
+    from bosss_b200 import replicas
+    mine = [specs[i] for i in replicas.shard(len(specs), ws, rank)]
+    procs = max(1, min(16, (os.cpu_count() or 2) // max(ws, 1) - 1))
+    pool = mp.get_context("spawn").Pool(procs)
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    from bosss_b200 import native as nat
+    from bosss_b200.batch import BatchSolver
+    nat.check(nat.lib().bsgpu_set_device(local))
+    t0 = time.perf_counter()
+    launches0 = nat.launch_count()
+    out = BatchSolver(lambda op: {"fast": _fgmres(op, PMG_SCHWARZ, True), "plain_fp64": _fgmres(op, PMG_BJ, False)},
+                      concurrency=args.concurrency).run(_bounded_imap(pool, _gen_xdg, mine, 2 * args.concurrency))
+    wall = time.perf_counter() - t0
+    launches = nat.launch_count() - launches0
+    pool.close()
+    fast, plain = out["fast"].as_dict(), out["plain_fp64"].as_dict()
+    agg = replicas.aggregate(fast["dof"], fast["solve_wall_s"], ws)
+    agg_plain = replicas.aggregate(plain["dof"], plain["solve_wall_s"], ws)
+    if rank != 0:
+        return
+    line = {
+        "metric": "aggregate DOF/s of a batch of independent XDG solves to 1e-10 (p50/p99 latency)",
+        "value": agg["per_s"], "unit": "DOF/s", "n_gpus": ws, "steps": 1, "warmup": 0,
+        "ms_per_step": agg["seconds"] * 1e3, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64 (outer) / f32 (preconditioner)", "data": "synthetic (seeded problems)",
+        "config": {"workload": f"{args.batch} {XDGBATCH}", "concurrency": args.concurrency, "tol": TOL,
+                   "parallelism": f"replicas x{ws} (problems sharded)", "host_generation_procs": procs},
+        "fast": fast, "plain_fp64": plain, "plain_fp64_dof_per_s": agg_plain["per_s"],
+        "speedup_vs_plain_fp64": agg["per_s"] / agg_plain["per_s"], "wall_s_incl_generation": wall,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_other_workload(args):
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps({"impl": "reference", "workload": args.workload,
+                              "unavailable": "the CPU reference arm is timed on the default workload only"}))
+        return
+    if args.workload == "xdgbatch":
+        return run_xdg_batch(args)
+    if args.workload == "xdg48":
+        from bosss_b200 import xdg
+        s = xdg.xdg_sphere(n=48, p=2, seed=args.seed)
+        return run_single_system(args, s, XDG48)
+    from bosss_b200 import assembly as A
+    s = A.variable_coeff_3d(96, 2, seed=args.seed)
+    feats = A.log_coeff_features(s)
+    nbr = s.grid.face_neighbours()
+    return run_single_system(args, s, VARCOEF96, prepare=lambda op: op.SetCellGraph(nbr, feats))
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.workload != "poisson64":
+        run_other_workload(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
-    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
-        import torch.distributed as dist
-        if dist.is_initialized():
-            dist.destroy_process_group()
+    from bosss_b200 import replicas
+    replicas.finalize(replicas.world()[0])
 
 
 if __name__ == "__main__":

@@ -613,6 +613,13 @@ class SineModes:
             out += term
         return out
 
+    def on_tensor_points(self, lo: np.ndarray, h: float, t1d: np.ndarray) -> np.ndarray:
+        """f on the tensor points lo_k + (t1d + 1) h / 2 of every cell k: [cells, n1, n1, n1] (x, y, z order),
+        from one sine table per direction."""
+        S = [np.sin(math.pi * self.k[None, :, d, None] * (lo[:, None, None, d] + (t1d[None, None, :] + 1) * (h / 2)))
+             for d in range(3)]                                                     # [cells, M, n1]
+        return np.einsum("m,kmi,kmj,kml->kijl", self.a, S[0], S[1], S[2], optimize=True)
+
     def project(self, grid: RectilinearGrid, p: int, q: Optional[int] = None) -> np.ndarray:
         """Separable projection: per mode and direction a 1-D Gauss integral, combined by outer products."""
         D = grid.D
@@ -682,6 +689,15 @@ def poisson_3d(n: int, p: int, seed: int = 0) -> BsrSystem:
     g = uniform_grid(3, n)
     rhs = SineModes.seeded(seed, 3).project(g, p)
     return assemble_sip(g, p, penalty=(p + 1) * (p + 2), rhs_cellwise=rhs)
+
+
+def log_coeff_features(system: BsrSystem) -> np.ndarray:
+    """[cells, 1 + 2D] float32: log nu of each cell and of its face neighbours (-x, +x, ...; the cell's own value
+    on the boundary) -- the per-cell input of the learned stage besides the residuals."""
+    nbr = system.grid.face_neighbours()
+    lk = np.log(np.ones(system.nb) if system.coeff is None else np.asarray(system.coeff, np.float64))
+    nb_lk = np.where(nbr >= 0, lk[np.maximum(nbr, 0)], lk[:, None])
+    return np.concatenate([lk[:, None], nb_lk], axis=1).astype(np.float32)
 
 
 def variable_coeff_3d(n: int, p: int, seed: int = 0, length: float = 0.1, variance: float = 1.0) -> BsrSystem:

@@ -397,7 +397,10 @@ BSGPU_API int bsgpu_solver_solve(bsgpu_solver_t s, double* X, const double* B, b
 BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats) {
   return guarded([&] {
     require(s && X && B, "null argument");
-    BSGPU_CUDA(cudaDeviceSynchronize());
+    // order after the caller's work on the legacy default stream only, so that solves driven from several host
+    // threads (one handle each) overlap on the device
+    BSGPU_CUDA(cudaEventRecord(s->e0, cudaStreamLegacy));
+    BSGPU_CUDA(cudaStreamWaitEvent(s->tree->ctx->st, s->e0, 0));
     solve_device(s, X, B, stats);
   });
 }

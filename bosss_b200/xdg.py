@@ -122,6 +122,10 @@ def xdg_sphere(n: int = 48, p: int = 2, seed: int = 0, mu=(1.0, 1000.0), radius=
                             T.append((a + x1 / sub, b + x2 / sub, cc + x3 / sub, wq[i1] * wq[i2] * wq[i3] / sub ** 3))
     T = np.asarray(T)
     tpts, tw = T[:, :3], T[:, 3]
+    nq1 = len(tq)
+    t1d = (sb[:, None] + tq[None, :] / sub).reshape(-1)        # the 1-D coordinates of the tensor point set
+    ga, gb, gc, g1, g2, g3 = np.indices((sub, sub, sub, nq1, nq1, nq1)).reshape(6, -1)
+    ixyz = ((ga * nq1 + g1) * len(t1d) + (gb * nq1 + g2)) * len(t1d) + (gc * nq1 + g3)   # point -> tensor index
     wvol = tw * (h / 2) ** 3
 
     # ---- classify cells: species fractions from the sub-cell points
@@ -168,10 +172,15 @@ def xdg_sphere(n: int = 48, p: int = 2, seed: int = 0, mu=(1.0, 1000.0), radius=
     diagU[cut] = 0.0
     offU = []                                              # (rows, cols, blocks) between uncut cells
     val_q, grad_q = _basis(p, modes, tpts, h)
-    for k in np.nonzero(cut)[0]:
-        for s in (0, 1):
-            sel = cut_sign[k] if s == 0 else ~cut_sign[k]
-            add(k, k, spc_off[s][k], spc_off[s][k], mu[s] * np.einsum("q,qad,qbd->ab", wvol * sel, grad_q, grad_q))
+    GG = np.einsum("qad,qbd->qab", grad_q, grad_q).reshape(len(wvol), Np * Np)
+    cut_list = np.nonzero(cut)[0]
+    if len(cut_list):
+        Wc = np.stack([cut_sign[k] for k in cut_list]) * wvol[None, :]         # [cut cells, q], species A
+        VA = (Wc @ GG).reshape(-1, Np, Np)
+        VB = ((wvol[None, :] - Wc) @ GG).reshape(-1, Np, Np)
+        for i, k in enumerate(cut_list):
+            add(k, k, spc_off[0][k], spc_off[0][k], mu[0] * VA[i])
+            add(k, k, spc_off[1][k], spc_off[1][k], mu[1] * VB[i])
     # load vector: uncut cells by the cell rule (separable for sine modes), cut cells per species by sub-cells
     from .assembly import project_function
     full = f.project(g, p) if isinstance(f, SineModes) else project_function(g, p, f, q=p + 4)
@@ -182,7 +191,10 @@ def xdg_sphere(n: int = 48, p: int = 2, seed: int = 0, mu=(1.0, 1000.0), radius=
     for k0 in range(0, len(cut_ids), 1024):
         K = cut_ids[k0:k0 + 1024]
         X = lo[K][:, None, :] + (tpts[None, :, :] + 1) * (h / 2)
-        fv = f([X[..., 0], X[..., 1], X[..., 2]])
+        if isinstance(f, SineModes):
+            fv = f.on_tensor_points(lo[K], h, t1d).reshape(len(K), -1)[:, ixyz]
+        else:
+            fv = f([X[..., 0], X[..., 1], X[..., 2]])
         inside = phi(X) < 0
         for s in (0, 1):
             sel = inside if s == 0 else ~inside
@@ -228,26 +240,32 @@ def xdg_sphere(n: int = 48, p: int = 2, seed: int = 0, mu=(1.0, 1000.0), radius=
         FLR = m[:, None, None] * (TLR[0][None] + e[:, None, None] * TLR[1][None])
         offU.append((kL, kR, FLR))
         offU.append((kR, kL, np.transpose(FLR, (0, 2, 1))))
-        for k, l, et in zip(Ls[~uu], Rs[~uu], eta[~uu]):
-            X = lo[k] + (tL + 1) * (h / 2)
-            ins = phi(X) < 0
+        # faces that touch a cut cell: all face rules of the direction as one product per species
+        kc, lc, ec = Ls[~uu], Rs[~uu], eta[~uu]
+        if len(kc):
+            q2 = lambda a_, b_: np.einsum("qa,qb->qab", a_, b_).reshape(len(wface), Np * Np)
+            Q = np.stack([q2(vL, dL) + q2(dL, vL), q2(vL, vL), q2(vL, dR), q2(dL, vR), q2(vL, vR),
+                          q2(vR, dR) + q2(dR, vR), q2(vR, vR)])                     # [7, q, Np^2]
+            insF = phi(lo[kc][:, None, :] + (tL[None] + 1) * (h / 2)) < 0           # [faces, q]
             for sp in (0, 1):
-                hk = hasA[k] if sp == 0 else hasB[k]
-                hl = hasA[l] if sp == 0 else hasB[l]
-                if not (hk and hl):
+                hk = hasA if sp == 0 else hasB
+                ok_f = hk[kc] & hk[lc]
+                Wf = wface[None, :] * (insF if sp == 0 else ~insF)
+                ok_f &= Wf.any(1)
+                if not ok_f.any():
                     continue
-                ww = wface * (ins if sp == 0 else ~ins)
-                if not ww.any():
-                    continue
+                T = np.einsum("fq,tqm->tfm", Wf[ok_f], Q).reshape(7, -1, Np, Np)
                 m_ = mu[sp]
-                ok, ol = spc_off[sp][k], spc_off[sp][l]
-                FLL = -0.5 * m_ * (o(vL, dL, ww) + o(dL, vL, ww)) + et * m_ * o(vL, vL, ww)
-                F = -0.5 * m_ * o(vL, dR, ww) + 0.5 * m_ * o(dL, vR, ww) - et * m_ * o(vL, vR, ww)
-                FRR = 0.5 * m_ * (o(vR, dR, ww) + o(dR, vR, ww)) + et * m_ * o(vR, vR, ww)
-                add(k, k, ok, ok, FLL)
-                add(l, l, ol, ol, FRR)
-                add(k, l, ok, ol, F)
-                add(l, k, ol, ok, F.T)
+                et = ec[ok_f][:, None, None]
+                FLL = -0.5 * m_ * T[0] + et * m_ * T[1]
+                F = -0.5 * m_ * T[2] + 0.5 * m_ * T[3] - et * m_ * T[4]
+                FRR = 0.5 * m_ * T[5] + et * m_ * T[6]
+                for i, (k, l) in enumerate(zip(kc[ok_f], lc[ok_f])):
+                    ok, ol = spc_off[sp][k], spc_off[sp][l]
+                    add(k, k, ok, ok, FLL[i])
+                    add(l, l, ol, ol, FRR[i])
+                    add(k, l, ok, ol, F[i])
+                    add(l, k, ol, ok, F[i].T)
         # Dirichlet boundary faces (the sphere never reaches them: uncut cells of the outer species only)
         for side in (-1.0, 1.0):
             Ks = np.nonzero(mi[d] == (0 if side < 0 else g.shape[d] - 1))[0]
@@ -286,12 +304,12 @@ def xdg_sphere(n: int = 48, p: int = 2, seed: int = 0, mu=(1.0, 1000.0), radius=
         w = wg[sel]
         eta = pen * cj[k] * max(muA, muB)
         sig = (1.0, -1.0)
+        VD = (v * w[:, None]).T @ dn
+        VV = (v * w[:, None]).T @ v
         for s in (0, 1):
             for tt in (0, 1):
                 ms, mt = mu[s], mu[tt]
-                M = (-0.5 * mt * sig[s] * np.einsum("q,qa,qb->ab", w, v, dn)
-                     - 0.5 * ms * sig[tt] * np.einsum("q,qa,qb->ab", w, dn, v)
-                     + eta * sig[s] * sig[tt] * np.einsum("q,qa,qb->ab", w, v, v))
+                M = -0.5 * mt * sig[s] * VD - 0.5 * ms * sig[tt] * VD.T + eta * sig[s] * sig[tt] * VV
                 add(k, k, spc_off[s][k], spc_off[tt][k], M)
 
     # ---- block-CSR with uneven blocks: uncut diagonal blocks (plus any sub-cell face terms of their cut
@@ -323,15 +341,35 @@ def xdg_sphere(n: int = 48, p: int = 2, seed: int = 0, mu=(1.0, 1000.0), radius=
     np.add.at(row_ptr, R_ + 1, 1)
     row_ptr = np.cumsum(row_ptr)
     col_idx = C_.astype(np.int32)
-    parts = []
-    for s_, i_ in zip(S_, I_):
-        if s_ == 0:
-            parts.append(diagU[i_].ravel())
-        elif s_ == 1:
-            parts.append(off_vals[i_].ravel())
-        else:
-            parts.append(blocks[dkeys[i_]].ravel())
-    values = np.concatenate(parts)
+    bsz = blen[R_].astype(np.int64) * blen[C_]
+    voff = np.concatenate([[0], np.cumsum(bsz)])
+    values = np.empty(int(voff[-1]))
+    ar = np.arange(Np * Np)
+    for src, arr in ((0, diagU), (1, off_vals)):
+        sel = np.nonzero(S_ == src)[0]
+        if len(sel):
+            values[voff[sel][:, None] + ar[None, :]] = arr[I_[sel]].reshape(len(sel), Np * Np)
+    for j in np.nonzero(S_ == 2)[0]:
+        values[voff[j]:voff[j + 1]] = blocks[dkeys[I_[j]]].ravel()
     species = np.stack([hasA, hasB], -1)
     return XdgSystem(Np=Np, nspc=nspc, species=species, row_ptr=row_ptr, col_idx=col_idx, values=values, rhs=rhs,
                      grid=g, p=p, centre=c, radius=R, mu=tuple(mu))
+
+
+BATCH_EDGES = (16, 24, 32, 40, 48)
+BATCH_JUMPS = (10.0, 100.0, 1000.0)
+
+
+def batch_specs(count: int = 256, seed: int = 0, p: int = 2) -> list:
+    """Seeded parameters of a batch of independent sphere problems: grid edge uniform in BATCH_EDGES, radius
+    uniform in [0.15, 0.35], centre uniform in [0.4, 0.6]^3, diffusivity jump 1:J with J uniform in BATCH_JUMPS,
+    and a per-problem seed of the right-hand side.  Each dict holds the keyword arguments of ``xdg_sphere``."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice(BATCH_EDGES))
+        R = float(rng.uniform(0.15, 0.35))
+        c = tuple(float(v) for v in rng.uniform(0.4, 0.6, size=3))
+        J = float(rng.choice(BATCH_JUMPS))
+        out.append(dict(n=n, p=p, seed=int(seed * 100003 + i), mu=(1.0, J), radius=R, centre=c))
+    return out

@@ -190,7 +190,9 @@ BSGPU_API int bsgpu_solver_destroy(bsgpu_solver_t s);
 /* ISolverSmootherTemplate.Solve via MultigridOperator.UseSolver: X (initial guess in, solution out) and B in the
  * original basis, host vectors.  Non-convergence is not an error (stats->converged = 0). */
 BSGPU_API int bsgpu_solver_solve(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats);
-/* Same with device vectors; synchronous on return. */
+/* Same with device vectors; synchronous on return.  The solve is ordered after work already queued on the legacy
+ * default stream; work on other streams that writes X or B must be complete before the call.  Handles are not
+ * thread-safe, but different handles may be driven from different host threads at the same time. */
 BSGPU_API int bsgpu_solver_solve_device(bsgpu_solver_t s, double* X, const double* B, bsgpu_solve_stats* stats);
 /* Residual-norm history of the last solve (outer iterations), up to cap entries. */
 BSGPU_API int bsgpu_solver_get_history(bsgpu_solver_t s, double* hist, int32_t cap, int32_t* n);

@@ -26,15 +26,20 @@ def test_schwarz_block_rows_match_oracle(cuda, Np, spc):
     assert np.abs(x - ref).max() <= 1e-10 * np.abs(ref).max()
 
 
-def test_schwarz_iterations_reduce_residual(cuda):
-    s = A.poisson_3d(5, 2)
-    op = MultigridOperator(BlockMsrMatrix.from_system(s))
-    r = []
-    for it in (1, 4):
-        x = np.zeros(s.N)
-        SchwarzConfig(FixedNoOfIterations=it).CreateInstance(op).Solve(x, s.rhs)
-        r.append(np.linalg.norm(s.rhs - s.to_scipy() @ x))
-    assert r[1] < 0.5 * r[0]
+def test_schwarz_iterations_match_oracle(cuda):
+    """FixedNoOfIterations updates x <- x + M (b - A x) (Schwarz.cs:1027-1047, restricted form) against the same
+    recursion on the oracle's patch inverses."""
+    v = random_var_bsr(50, 4, seed=31, max_spc=2, nnz_per_row=3, spd=True)
+    Bo = O.Bsr.of(v)
+    Mo = O.Bsr.of(v, values=O.schwarz_rows(Bo))
+    x = np.zeros(v.N)
+    for _ in range(3):
+        r = O.spmv(Bo, -1.0, x, 1.0, v.rhs.copy())
+        x = O.spmv(Mo, 1.0, r, 1.0, x.copy())
+    op = MultigridOperator(BlockMsrMatrix.from_system(v), MultigridOperator.Eye)
+    got = np.zeros(v.N)
+    SchwarzConfig(FixedNoOfIterations=3).CreateInstance(op).Solve(got, v.rhs)
+    assert np.abs(got - x).max() <= 1e-10 * np.abs(x).max()
 
 
 def test_schwarz_rejects_unsupported_overlap(cuda):
@@ -86,3 +91,27 @@ def test_xdg_spmv_matches_oracle(cuda):
     got = yv.copy()
     M.SpMV(0.7, xv, -0.3, got)
     assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_batch_of_independent_xdg_problems(cuda):
+    """Waves of concurrently solved problems (one handle and stream each) give the same solutions as the direct
+    solve of every problem."""
+    from bosss_b200.batch import BatchSolver
+    specs = [dict(n=n, p=1, seed=i, mu=(1.0, J), radius=r, centre=(0.5, 0.48, 0.52))
+             for i, (n, J, r) in enumerate([(6, 10.0, 0.3), (8, 100.0, 0.25), (6, 1000.0, 0.2), (7, 10.0, 0.33),
+                                            (8, 1000.0, 0.3)])]
+    systems = [xdg.xdg_sphere(**sp) for sp in specs]
+    pmg = PmgConfig(DegreeHierarchy=(4, 1), Smoother="schwarz", NoOfPostSmootherSweeps=2, CoarseTolerance=1e-2,
+                    CoarseMaxIterations=200)
+    make = lambda op, mixed: FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative",
+                                          Preconditioners=[pmg], MixedPrecision=mixed).CreateInstance(op)
+    sols = {}
+    out = BatchSolver(lambda op: {"mixed": make(op, True), "fp64": make(op, False)}, concurrency=2).run(
+        systems, on_result=lambda name, r, w: sols.__setitem__((name, r.index), w["X"][name].cpu().numpy()))
+    assert set(out) == {"mixed", "fp64"}
+    for summary in out.values():
+        assert len(summary.results) == 5 and summary.as_dict()["all_converged"]
+    for i, s in enumerate(systems):
+        xd = O.direct_solve(s)
+        for name in out:
+            assert np.linalg.norm(sols[(name, i)] - xd) <= SOL_TOL * np.linalg.norm(xd)
