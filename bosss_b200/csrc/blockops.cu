@@ -353,6 +353,74 @@ __global__ void schwarz_factor_kernel(const int64_t* __restrict__ rp, const int3
   }
 }
 
+// Block ILU(0) of a two-colour block graph with the rows ordered colour 0 first (CellILU.ComputeILU,
+// CellILU.cs:1229-1330, applied to the reordered matrix).  Colour-0 rows have no lower neighbours, so their
+// factors are A's blocks (copied beforehand); every colour-1 row b only has colour-0 neighbours r, hence
+//   L_br = A_br A_rr^{-1},   U_bb = A_bb - sum_r L_br A_rb,
+// and no other block of the pattern changes.  One CTA per colour-1 row; dinv: A_rr^{-1}, column-major per block
+// row at doff.  M (FP64, A's structure and layout) receives L_br and U_bb.
+__global__ void ilu0_two_colour_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                       const int32_t* __restrict__ len, const int64_t* __restrict__ boff,
+                                       const double* __restrict__ vals, int V, const int64_t* __restrict__ doff,
+                                       const double* __restrict__ dinv, const int32_t* __restrict__ rows,
+                                       int64_t nrows, double* __restrict__ M, int* __restrict__ err) {
+  extern __shared__ double sm[];
+  for (int64_t q = blockIdx.x; q < nrows; q += gridDim.x) {
+    const int64_t b = rows[q];
+    const int I = len[b];
+    double* U = sm;            // I x I row-major
+    double* L = sm + I * I;    // I x J row-major (J <= max block length)
+    int64_t kd = -1;
+    for (int64_t k = rp[b]; k < rp[b + 1]; ++k)
+      if (ci[k] == b) kd = k;
+    if (kd < 0) {
+      if (threadIdx.x == 0) atomicCAS(err, 0, (int)(b + 1 < 0x7fffffff ? b + 1 : 0x7fffffff));
+      continue;
+    }
+    for (int e = threadIdx.x; e < I * I; e += blockDim.x) {
+      const int r = e / I, c = e - r * I;
+      U[e] = vals[boff[kd] + (int64_t)(c / V) * I * V + r * V + (c % V)];
+    }
+    __syncthreads();
+    for (int64_t k = rp[b]; k < rp[b + 1]; ++k) {
+      const int64_t r = ci[k];
+      if (r == b) continue;
+      const int J = len[r];
+      // block (r, b) in row r (structurally symmetric pattern)
+      int64_t krb = -1;
+      for (int64_t t = rp[r]; t < rp[r + 1]; ++t)
+        if (ci[t] == b) krb = t;
+      if (krb < 0) {
+        if (threadIdx.x == 0) atomicCAS(err, 0, (int)(b + 1 < 0x7fffffff ? b + 1 : 0x7fffffff));
+        break;
+      }
+      const double* D = dinv + doff[r];
+      for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+        const int i = e / J, c = e - i * J;
+        double acc = 0.0;
+        for (int p = 0; p < J; ++p)
+          acc = fma(vals[boff[k] + (int64_t)(p / V) * I * V + i * V + (p % V)], D[c * J + p], acc);
+        L[e] = acc;
+        M[boff[k] + (int64_t)(c / V) * I * V + i * V + (c % V)] = acc;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < I * I; e += blockDim.x) {
+        const int i = e / I, c = e - i * I;
+        double acc = 0.0;
+        for (int p = 0; p < J; ++p)
+          acc = fma(L[i * J + p], vals[boff[krb] + (int64_t)(c / V) * J * V + p * V + (c % V)], acc);
+        U[e] -= acc;
+      }
+      __syncthreads();
+    }
+    for (int e = threadIdx.x; e < I * I; e += blockDim.x) {
+      const int r = e / I, c = e - r * I;
+      M[boff[kd] + (int64_t)(c / V) * I * V + r * V + (c % V)] = U[e];
+    }
+    __syncthreads();
+  }
+}
+
 DBuf<int32_t> blk_rows(const Matrix& A) {
   std::vector<int32_t> br(A.nnzb);
   for (int64_t i = 0; i < A.nb; ++i)
@@ -401,6 +469,21 @@ void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cuda
   if (smem > 48 * 1024) BSGPU_CUDA(cudaFuncSetAttribute(invert_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   invert_kernel<<<grid_for(A.nb), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, A.doff.p, D64, D32,
                                                   err, A.nb);
+  BSGPU_CHECK_LAUNCH();
+}
+
+void ilu0_two_colour(const Matrix& A, const double* dinv, const int32_t* rows1, int64_t n1, Matrix& M, int* err,
+                     cudaStream_t st) {
+  require(!A.single && !M.single && M.V == A.V && M.nvals == A.nvals, "ILU(0) factors need FP64 matrices");
+  BSGPU_CUDA(cudaMemcpyAsync(M.v64.p, A.v64.p, (size_t)A.nvals * 8, cudaMemcpyDeviceToDevice, st));
+  if (n1 == 0) return;
+  const int64_t n = A.max_len();
+  const size_t smem = (size_t)(2 * n * n) * sizeof(double);
+  require(smem <= 200 * 1024, "block too large for ILU(0)", BSGPU_ERR_UNSUPPORTED);
+  if (smem > 48 * 1024)
+    BSGPU_CUDA(cudaFuncSetAttribute(ilu0_two_colour_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ilu0_two_colour_kernel<<<grid_for(n1), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, A.doff.p,
+                                                          dinv, rows1, n1, M.v64.p, err);
   BSGPU_CHECK_LAUNCH();
 }
 

@@ -17,6 +17,11 @@ void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cuda
 // (Schwarz.cs:623-840 block set-up; blocks here are cell patches with overlap 1).  One launch for all blocks,
 // whatever their sizes.
 void schwarz_factor(const Matrix& A, Matrix& M, int* err, cudaStream_t st);
+// Block ILU(0) of a two-colour block graph, rows ordered colour 0 first (CellILU.cs:1229-1330 on the reordered
+// matrix): M (FP64, A's structure) <- A with L_br = A_br A_rr^{-1} and U_bb = A_bb - sum_r L_br A_rb on the
+// colour-1 rows `rows1`.  dinv: inverses of A's diagonal blocks (invert_diag_blocks layout).
+void ilu0_two_colour(const Matrix& A, const double* dinv, const int32_t* rows1, int64_t n1, Matrix& M, int* err,
+                     cudaStream_t st);
 // y_i = L_i^{-T} x_i per block (initial-guess transform with a lower-triangular L, row-major).
 void block_trsv_lt(const Matrix& A, const double* L, const double* x, double* y, cudaStream_t st);
 

@@ -188,6 +188,68 @@ struct BlockGST : Solver<T> {
   }
 };
 
+// Block ILU(0) smoother (CellILU, CellILU.cs:22; factorisation :1229-1330, Solve :182-250 with the
+// single-precision back substitution of BackSubs_Optimized_SinglePrec :914).  The reference factors the cells in
+// their natural order, a chain of dependencies as long as the grid is wide; here the cells are ordered by the two
+// colours of the block graph (faces of a Cartesian or cut-cell grid: parity of the cell index), which makes the
+// factorisation one launch and x = U^{-1} L^{-1} b two block Gauss-Seidel-type launches over the colours:
+//   x <- b;  x_b <- U_bb^{-1} (b_b - sum_r L_br x_r)  (colour 1);  x_r <- A_rr^{-1} (b_r - sum_b A_rb x_b)  (colour 0)
+// (with M_ii = U_ii the in-place update x_i + U_ii^{-1}(b_i - sum_j M_ij x_j) is exactly that).  Factors in FP32
+// for the mixed-precision preconditioner.
+template <typename T>
+struct ILU0T : Solver<T> {
+  std::unique_ptr<Matrix> M64, M32;
+  const Matrix* M = nullptr;
+  DBuf<T> uinv;
+  DBuf<int32_t> rows[2];
+  int64_t cnt[2] = {0, 0};
+  ILU0T(Ctx& c, const Matrix* A64) {
+    require(A64->uniform && (A64->Np == 4 || A64->Np == 6 || A64->Np == 10 || A64->Np == 20),
+            "ILU smoother needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
+    auto cols = greedy_colouring(*A64);
+    require(cols.size() <= 2, "ILU smoother needs a two-colour block graph (" + std::to_string(cols.size()) +
+                                  " colours)", BSGPU_ERR_UNSUPPORTED);
+    for (size_t k = 0; k < cols.size(); ++k) {
+      cnt[k] = (int64_t)cols[k].size();
+      rows[k].alloc(std::max<int64_t>(cnt[k], 1));
+      if (cnt[k]) BSGPU_CUDA(cudaMemcpy(rows[k].p, cols[k].data(), cnt[k] * 4, cudaMemcpyHostToDevice));
+    }
+    std::vector<int64_t> o = diag_offsets(*A64);
+    DBuf<double> dinv(std::max<int64_t>(o.back(), 1));
+    int* err = c.flag();
+    invert_diag_blocks(*A64, dinv.p, nullptr, err, c.st);
+    c.check_flag(err, "ILU: singular diagonal block");
+    M64.reset(matrix_like(*A64, false));
+    err = c.flag();
+    ilu0_two_colour(*A64, dinv.p, rows[1].p, cnt[1], *M64, err, c.st);
+    c.check_flag(err, "ILU: block pattern is not structurally symmetric");
+    uinv.alloc(std::max<int64_t>(o.back(), 1));
+    err = c.flag();
+    if constexpr (sizeof(T) == 8)
+      invert_diag_blocks(*M64, uinv.p, nullptr, err, c.st);
+    else
+      invert_diag_blocks(*M64, nullptr, uinv.p, err, c.st);
+    c.check_flag(err, "ILU: singular pivot block");
+    if constexpr (sizeof(T) == 4) {
+      M32.reset(matrix_to_single(*M64, c.st));
+      BSGPU_CUDA(cudaStreamSynchronize(c.st));
+      M64.reset();
+      M = M32.get();
+    } else {
+      M = M64.get();
+    }
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    (void)zero;  // CellILU overwrites X
+    TraceScope ts(c, this->trace);
+    copy_vec(X, B, M->N, c.st);
+    if (cnt[1]) gs_update_rows(*M, uinv.p, T(1), rows[1].p, cnt[1], B, X, c.st);
+    if (cnt[0]) gs_update_rows(*M, uinv.p, T(1), rows[0].p, cnt[0], B, X, c.st);
+    this->this_level_iterations++;
+    this->converged = true;
+  }
+};
+
 // Additive Schwarz smoother (Schwarz.cs:56; Init :623-840, Solve :996-1147) in restricted form with one
 // overlapping block per cell (schwarz_factor in blockops.cu): x <- x + M (b - A x), M holding the centre rows of
 // the block inverses, stored in FP32 for the mixed-precision preconditioner.  bj_iters + 1 updates per call, as
@@ -1133,6 +1195,7 @@ std::unique_ptr<Solver<T>> build_hlevel(Tree& t, const Matrix* A64, const Matrix
   ht.mode = 2;
   ht.max_iter = std::max(1, cfg.h_cycle);
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
+  omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = cfg.h_sweeps;
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -1158,6 +1221,9 @@ std::unique_ptr<Solver<T>> make_smoother(Ctx& c, const Matrix* A64, const Matrix
   } else if (kind == BSGPU_SMOOTHER_SCHWARZ) {
     s = std::make_unique<SchwarzT<T>>(c, A64, AT, cfg.bj_iters);
     tag = ".Schwarz";
+  } else if (kind == BSGPU_SMOOTHER_ILU) {
+    s = std::make_unique<ILU0T<T>>(c, A64);
+    tag = ".CellILU";
   } else {
     s = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
   }
@@ -1200,6 +1266,7 @@ std::unique_ptr<Solver<T>> build_hmg_level(Tree& t, const HmgHierarchy* H, const
     ht.max_iter = std::max(1, cfg.h_cycle);
   }
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
+  omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = std::max(1, cfg.h_sweeps);
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -1262,6 +1329,7 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   }
   const std::string lv = "L" + std::to_string(level);
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
+  omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->trace = c.trace_id(lv + ".OrthoMG");
   if (level == 0 && t.net && (cfg.learned & BSGPU_LEARNED_PRESMOOTH)) {
     omg->pre = std::make_unique<LearnedPrecondT<T>>(c, t.net.get());

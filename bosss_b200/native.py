@@ -17,7 +17,7 @@ SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI = 0, 1, 2,
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS, SMOOTHER_SCHWARZ = 0, 1, 2
+SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS, SMOOTHER_SCHWARZ, SMOOTHER_ILU = 0, 1, 2, 3
 LEARNED_OFF, LEARNED_FGMRES, LEARNED_PRESMOOTH, LEARNED_BOTH = 0, 1, 2, 3
 
 # every symbol the header declares (checked by the CPU test-suite)
@@ -44,7 +44,7 @@ class SolverConfig(C.Structure):
                 ("precision", C.c_int32), ("h_levels", C.c_int32), ("h_sweeps", C.c_int32), ("h_cycle", C.c_int32),
                 ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
                 ("learned", C.c_int32), ("learned_hidden", C.c_int32), ("learned_stall", C.c_double),
-                ("reserved", C.c_int32 * 6)]
+                ("ortho_max_krylov", C.c_int32), ("reserved", C.c_int32 * 5)]
 
 
 class SolveStats(C.Structure):

@@ -211,7 +211,12 @@ class IterativeSolverConfig:
 
 @dataclass
 class PmgConfig(IterativeSolverConfig):
-    """PmgConfig.CreateInstanceImpl__Kummer with UseILU = false (block-Jacobi post-smoother on every level).
+    """PmgConfig.CreateInstanceImpl__Kummer (PmgConfig.cs:80-245).
+
+    Post-smoother of every p-level: ``UseILU = True`` selects block ILU(0) (CellILU, as PmgConfig.cs:124-141 does
+    for the levels it creates; here the cells are ordered by the two colours of the block graph), otherwise
+    ``Smoother``: "blockjacobi" (BlockJacobi with ``BlockJacobiIterations``), "blockgs" (symmetric multicolour
+    block Gauss-Seidel), "schwarz" (restricted additive Schwarz, one patch per cell) or "ilu".
 
     ``DegreeHierarchy``: modes per species kept on each level, finest first (e.g. (20, 10, 4) for p = 3 -> 2 -> 1
     in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative), by CG
@@ -239,11 +244,10 @@ class PmgConfig(IterativeSolverConfig):
     DenseLimit: int = 1024
     Smoother: str = "blockjacobi"
     HSmoother: str = "blockjacobi"
+    OrthoMaxKrylovDim: int = 96     # OrthonormalizationMultigrid.Config.MaxKrylovDim: history length per level
     UseILU: bool = False
 
     def _fill(self, c):
-        if self.UseILU:
-            raise NotImplementedError("CellILU smoothing is not available; set UseILU = False")
         c.n_levels = len(self.DegreeHierarchy)
         for i, k in enumerate(self.DegreeHierarchy):
             c.level_keep[i] = int(k)
@@ -263,11 +267,14 @@ class PmgConfig(IterativeSolverConfig):
         c.h_cycle = self.HCycle
         c.dense_limit = self.DenseLimit
         sm = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "blockgs": nat.SMOOTHER_BLOCKGS,
-              "schwarz": nat.SMOOTHER_SCHWARZ}
+              "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU}
         if self.Smoother not in sm or self.HSmoother not in sm:
             raise ValueError(f"Smoother / HSmoother must be one of {sorted(sm)}")
-        c.smoother = sm[self.Smoother]
+        c.smoother = nat.SMOOTHER_ILU if self.UseILU else sm[self.Smoother]
         c.h_smoother = sm[self.HSmoother]
+        if self.OrthoMaxKrylovDim < 2:
+            raise ValueError("OrthoMaxKrylovDim must be at least 2")
+        c.ortho_max_krylov = self.OrthoMaxKrylovDim
 
     def _config(self):
         c = self._base()
@@ -332,6 +339,24 @@ class BlockJacobiConfig:
         c.solver = nat.SOLVER_BLOCKJACOBI
         c.bj_iters = self.NoOfIterations
         c.bj_omega = self.omega
+        return GpuSolver(op, c)
+
+
+@dataclass
+class CellILUConfig:
+    """CellILU (CellILU.cs:22) with ILU_level = 0 as a stand-alone solver: X = U^{-1} L^{-1} B per call.
+
+    The block ILU(0) factors are computed for the cells ordered by the two colours of the block graph (the
+    reference uses the natural order); blocks must be uniform of size 4, 6, 10 or 20."""
+    ILU_level: int = 0
+
+    def CreateInstance(self, op: MultigridOperator) -> "GpuSolver":
+        if self.ILU_level != 0:
+            raise NotImplementedError("only ILU_level = 0 is available")
+        c = nat.SolverConfig()
+        nat.check(nat.lib().bsgpu_solver_config_default(C.byref(c)))
+        c.solver = nat.SOLVER_BLOCKJACOBI
+        c.smoother = nat.SMOOTHER_ILU
         return GpuSolver(op, c)
 
 

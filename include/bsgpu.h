@@ -137,7 +137,9 @@ enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in 
  * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20), or
  * restricted additive Schwarz with one overlapping block per cell (Schwarz.cs:56; bj_iters + 1 updates; blocks
  * of up to ~160 unknowns, uneven sizes allowed), factors in FP32 for the mixed-precision preconditioner */
-enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1, BSGPU_SMOOTHER_SCHWARZ = 2 };
+enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1, BSGPU_SMOOTHER_SCHWARZ = 2,
+       BSGPU_SMOOTHER_ILU = 3 /* block ILU(0) (CellILU.cs:22, PmgConfig UseILU), cells ordered by the two colours
+                                 of the block graph; uniform blocks of 4, 6, 10 or 20 */ };
 /* learned preconditioner stage (no counterpart in the reference): a one-hop message-passing MLP over the cell
  * graph, BF16 weights, FP32 accumulation.  FGMRES: an extra FlexGMRES preconditioner used in turn with the
  * p-multigrid V-cycle (FlexGMRES.cs:196-199 round-robin); PRESMOOTH: pre-smoother of the finest OrthoMG level
@@ -172,7 +174,10 @@ typedef struct {
   int32_t learned_hidden;   /* hidden width of the learned stage (multiple of 16, default 64)   */
   double learned_stall;     /* a learned step reducing the residual by less than this factor
                                switches the stage off for the rest of the solve (default 0.99)  */
-  int32_t reserved[6];
+  int32_t ortho_max_krylov; /* OrthoMG history length (OrthonormalizationMultigrid.Config.MaxKrylovDim,
+                               OrthonormalizationMultigrid.cs:486); when full, the minimisation restarts from
+                               the current iterate (default 96)                                  */
+  int32_t reserved[5];
 } bsgpu_solver_config;
 
 typedef struct {

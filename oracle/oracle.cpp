@@ -863,6 +863,122 @@ int or_schwarz_rows(const or_bsr* m, double* values_out) {
   }
 }
 
+// Block ILU(0) (CellILU.ComputeILU, CellILU.cs:1229-1330, ILU_level = 0 as PmgConfig.cs:131 sets it): Saad's
+// in-place KIJ form over the block rows taken in the order `order` (NULL: natural order, the reference's).
+// factor_out receives the factors in A's layout: strictly lower blocks L_ik (unit lower factor), upper blocks and
+// the diagonal U_ij.  A diagonal block whose factorisation fails is skipped, as the reference does.
+namespace {
+void gemm_sub(int I, int K, int J, const double* A, const double* B, double* C) {  // C -= A B, row-major
+  for (int r = 0; r < I; ++r)
+    for (int k = 0; k < K; ++k) {
+      const double a = A[r * K + k];
+      for (int c = 0; c < J; ++c) C[r * J + c] -= a * B[k * J + c];
+    }
+}
+int64_t find_block(const Mat& A, int64_t i, int32_t j) {
+  const int32_t* b = A.ci.data() + A.rp[i];
+  const int32_t* e = A.ci.data() + A.rp[i + 1];
+  const int32_t* p = std::lower_bound(b, e, j);
+  return (p != e && *p == j) ? A.rp[i] + (p - b) : -1;
+}
+std::vector<int64_t> positions(const Mat& A, const int32_t* order) {
+  std::vector<int64_t> pos(A.nb);
+  for (int64_t q = 0; q < A.nb; ++q) pos[order ? order[q] : q] = q;
+  return pos;
+}
+}  // namespace
+
+int or_ilu0_factor(const or_bsr* m, const int32_t* order, double* factor_out) {
+  try {
+    Mat A;
+    load_mat(A, m);
+    std::vector<int64_t> pos = positions(A, order);
+    std::copy(A.val, A.val + A.vp[A.nnzb()], factor_out);
+    auto W = [&](int64_t k) { return factor_out + A.vp[k]; };
+    for (int64_t kk = 0; kk + 1 < A.nb; ++kk) {
+      const int64_t k = order ? order[kk] : kk;
+      const int Sk = A.len[k];
+      if (Sk == 0) continue;
+      const int64_t dkk = find_block(A, k, (int32_t)k);
+      if (dkk < 0) continue;
+      std::vector<double> inv(W(dkk), W(dkk) + (size_t)Sk * Sk);
+      if (invert(Sk, inv.data()) != 0) continue;
+      // rows i > k (in the ordering) with an occupied block (i, k); the pattern is structurally symmetric
+      for (int64_t q = A.rp[k]; q < A.rp[k + 1]; ++q) {
+        const int64_t i = A.ci[q];
+        if (pos[i] <= pos[k]) continue;
+        const int64_t qik = find_block(A, i, (int32_t)k);
+        if (qik < 0) continue;
+        const int Si = A.len[i];
+        std::vector<double> L((size_t)Si * Sk, 0.0);
+        gemm_sub(Si, Sk, Sk, W(qik), inv.data(), L.data());          // L = -A_ik inv(A_kk)
+        for (auto& v : L) v = -v;
+        std::copy(L.begin(), L.end(), W(qik));
+        for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+          const int32_t j = A.ci[p];
+          if (pos[j] <= pos[k]) continue;
+          const int64_t qkj = find_block(A, k, j);
+          if (qkj < 0) continue;                                      // (k, j) outside the ILU(0) pattern
+          gemm_sub(Si, Sk, A.len[j], L.data(), W(qkj), W(p));
+        }
+      }
+    }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return OR_ERR_ARGUMENT;
+  }
+}
+
+// x = U^{-1} L^{-1} b with the factors of or_ilu0_factor (CellILU.Solve, CellILU.cs:182-250: LoTriDiagonalSolve
+// with the unit lower factor, then UpTriDiagonalSolve with the upper factor and its diagonal blocks).
+int or_ilu0_solve(const or_bsr* m, const int32_t* order, const double* factor, const double* b, double* x) {
+  try {
+    Mat A;
+    load_mat(A, m);
+    std::vector<int64_t> pos = positions(A, order);
+    std::vector<double> y(b, b + A.N);
+    for (int64_t q = 0; q < A.nb; ++q) {
+      const int64_t i = order ? order[q] : q;
+      const int I = A.len[i];
+      for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+        const int32_t k = A.ci[p];
+        if (pos[k] >= pos[i]) continue;
+        const int K = A.len[k];
+        const double* L = factor + A.vp[p];
+        for (int r = 0; r < I; ++r)
+          for (int c = 0; c < K; ++c) y[A.i0[i] + r] -= L[r * K + c] * y[A.i0[k] + c];
+      }
+    }
+    for (int64_t q = A.nb - 1; q >= 0; --q) {
+      const int64_t i = order ? order[q] : q;
+      const int I = A.len[i];
+      std::vector<double> s(y.begin() + A.i0[i], y.begin() + A.i0[i] + I);
+      for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+        const int32_t j = A.ci[p];
+        if (pos[j] <= pos[i]) continue;
+        const int J = A.len[j];
+        const double* U = factor + A.vp[p];
+        for (int r = 0; r < I; ++r)
+          for (int c = 0; c < J; ++c) s[r] -= U[r * J + c] * x[A.i0[j] + c];
+      }
+      const int64_t d = find_block(A, i, (int32_t)i);
+      if (d < 0) { g_err = "ILU: missing diagonal block"; return OR_ERR_ARGUMENT; }
+      std::vector<double> inv(factor + A.vp[d], factor + A.vp[d] + (size_t)I * I);
+      if (invert(I, inv.data()) != 0) { g_err = "ILU: singular diagonal block"; return OR_ERR_ARITHMETIC; }
+      for (int r = 0; r < I; ++r) {
+        double acc = 0.0;
+        for (int c = 0; c < I; ++c) acc += inv[r * I + c] * s[c];
+        x[A.i0[i] + r] = acc;
+      }
+    }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return OR_ERR_ARGUMENT;
+  }
+}
+
 int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const double* b) {
   try {
     Mat A;

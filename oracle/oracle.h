@@ -50,6 +50,9 @@ int or_change_of_basis(const or_bsr* m, double* values_out, double* L_out);
 int or_restrict(const or_bsr* m, int keep, double* values_out, int64_t* map_out);
 int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const double* b);
 int or_schwarz_rows(const or_bsr* m, double* values_out);
+/* block ILU(0) over the block rows in `order` (NULL: natural order); factors in the matrix layout */
+int or_ilu0_factor(const or_bsr* m, const int32_t* order, double* factor_out);
+int or_ilu0_solve(const or_bsr* m, const int32_t* order, const double* factor, const double* b, double* x);
 int or_solve(const or_bsr* m, const or_solver_cfg* c, const double* b, double* x, or_stats* stats, double* hist,
              int hist_cap);
 /* persistent solver (set-up once, many solves); the matrix arrays must outlive it */

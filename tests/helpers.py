@@ -136,3 +136,17 @@ def sip_cartesian1():
                        boundary=lambda d, side, x: (d == 0) & (side < 0) & np.ones_like(x[0], bool),
                        rhs_f=lambda X: -np.ones_like(X[0]))
     return g, s, (lambda X: 0.5 * X[0] ** 2 - 10 * X[0])
+
+
+def greedy_colour_order(row_ptr, col_idx) -> np.ndarray:
+    """Block rows ordered by the greedy colouring of the block graph in natural order (colour 0 first), the
+    order the GPU block ILU(0) factors in."""
+    nb = len(row_ptr) - 1
+    col = np.full(nb, -1)
+    for i in range(nb):
+        used = {col[j] for j in col_idx[row_ptr[i]:row_ptr[i + 1]] if j != i and col[j] >= 0}
+        c = 0
+        while c in used:
+            c += 1
+        col[i] = c
+    return np.concatenate([np.nonzero(col == c)[0] for c in range(col.max() + 1)]).astype(np.int32)

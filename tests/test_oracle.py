@@ -160,3 +160,33 @@ def test_blockjacobi_two_updates():
     x1 = Di @ v.rhs
     x2 = x1 + Di @ (v.rhs - M @ x1)
     assert np.abs(x - x2).max() < 1e-12 * np.abs(x2).max()
+
+
+@pytest.mark.parametrize("ordered", [False, True])
+def test_ilu0_reproduces_the_matrix_on_its_pattern(ordered):
+    """Defining property of ILU(0) (CellILU.ComputeILU, Saad's in-place form): (L U)_ij = A_ij on every occupied
+    block, L unit lower and U upper in the factorisation order; the solve applies (L U)^{-1}."""
+    from helpers import greedy_colour_order
+    s = A.poisson_3d(3, 1, seed=4)
+    order = greedy_colour_order(s.row_ptr, s.col_idx) if ordered else np.arange(s.nb, dtype=np.int32)
+    Bo = O.Bsr.of(s)
+    F = O.ilu0_factor(Bo, order if ordered else None).reshape(-1, s.Np, s.Np)
+    pos = np.empty(s.nb, np.int64)
+    pos[order] = np.arange(s.nb)
+    Np, N = s.Np, s.N
+    L, U = np.eye(N), np.zeros((N, N))
+    pattern = np.zeros((N, N), bool)
+    for i in range(s.nb):
+        for q in range(s.row_ptr[i], s.row_ptr[i + 1]):
+            j = s.col_idx[q]
+            sl = np.s_[i * Np:(i + 1) * Np, j * Np:(j + 1) * Np]
+            pattern[sl] = True
+            if pos[j] < pos[i]:
+                L[sl] = F[q]
+            else:
+                U[sl] = F[q]
+    Ad = s.to_scipy().toarray()
+    assert np.abs((L @ U - Ad)[pattern]).max() <= 1e-12 * np.abs(Ad).max()
+    b = np.random.default_rng(1).standard_normal(N)
+    x = O.ilu0_solve(Bo, F.reshape(-1), b, order if ordered else None)
+    assert np.abs(L @ U @ x - b).max() <= 1e-10 * np.abs(b).max()
