@@ -155,6 +155,49 @@ void axpys_impl(int K, const double* dcoef, const double* hcoef, double sign, co
   }
 }
 
+// The same coefficients applied to two vector sets in one pass: y1 += sign*sum c_k x1_k, y2 += sign*sum c_k x2_k
+// (the Gram-Schmidt update of a correction and of its image under the operator).
+template <typename T>
+struct Axpy2Args {
+  const T* x1[kMaxAxpy];
+  const T* x2[kMaxAxpy];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads) axpys2_kernel(Axpy2Args<T> args, const double* __restrict__ dcoef, int K,
+                                                          double sign, T* __restrict__ y1, T* __restrict__ y2,
+                                                          int64_t n) {
+  __shared__ double c[kMaxAxpy];
+  if (threadIdx.x < K) c[threadIdx.x] = sign * dcoef[threadIdx.x];
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+    double a1 = 0.0, a2 = 0.0;
+    for (int k = 0; k < K; ++k) {
+      a1 = fma(c[k], (double)args.x1[k][i], a1);
+      a2 = fma(c[k], (double)args.x2[k][i], a2);
+    }
+    y1[i] = (T)((double)y1[i] + a1);
+    y2[i] = (T)((double)y2[i] + a2);
+  }
+}
+
+template <typename T>
+void axpys2_impl(int K, const double* dcoef, double sign, const T* const* x1, T* y1, const T* const* x2, T* y2,
+                 int64_t n, cudaStream_t st) {
+  if (n == 0 || K == 0) return;
+  const int grid = (int)std::min<int64_t>((n + kThreads - 1) / kThreads, (int64_t)num_sms() * 8);
+  for (int k0 = 0; k0 < K; k0 += kMaxAxpy) {
+    const int kc = std::min(kMaxAxpy, K - k0);
+    Axpy2Args<T> args{};
+    for (int k = 0; k < kc; ++k) {
+      args.x1[k] = x1[k0 + k];
+      args.x2[k] = x2[k0 + k];
+    }
+    axpys2_kernel<T><<<grid, kThreads, 0, st>>>(args, dcoef + k0, kc, sign, y1, y2, n);
+    BSGPU_CHECK_LAUNCH();
+  }
+}
+
 template <typename T>
 __global__ void scale_inv2_kernel(const double* __restrict__ d, T* __restrict__ x, T* __restrict__ y, int64_t n,
                                   int* __restrict__ err, const int* __restrict__ active) {
@@ -276,6 +319,14 @@ void axpys(int K, const double* dcoef, const double* hcoef, double sign, const d
 void axpys(int K, const double* dcoef, const double* hcoef, double sign, const float* const* x, float* y, int64_t n,
            cudaStream_t st, const int* active) {
   axpys_impl<float>(K, dcoef, hcoef, sign, x, y, n, st, active);
+}
+void axpys2(int K, const double* dcoef, double sign, const double* const* x1, double* y1, const double* const* x2,
+            double* y2, int64_t n, cudaStream_t st) {
+  axpys2_impl<double>(K, dcoef, sign, x1, y1, x2, y2, n, st);
+}
+void axpys2(int K, const double* dcoef, double sign, const float* const* x1, float* y1, const float* const* x2,
+            float* y2, int64_t n, cudaStream_t st) {
+  axpys2_impl<float>(K, dcoef, sign, x1, y1, x2, y2, n, st);
 }
 void scale_inv2(const double* d, double* x, double* y, int64_t n, int* err, cudaStream_t st, const int* active) {
   if (n == 0) return;

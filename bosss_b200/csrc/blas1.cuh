@@ -32,6 +32,12 @@ void axpys(int K, const double* dcoef, const double* hcoef, double sign, const d
 void axpys(int K, const double* dcoef, const double* hcoef, double sign, const float* const* x, float* y, int64_t n,
            cudaStream_t st, const int* active = nullptr);
 
+// y1 += sign * sum_k dcoef[k] * x1[k][i] and y2 += sign * sum_k dcoef[k] * x2[k][i] in one pass.
+void axpys2(int K, const double* dcoef, double sign, const double* const* x1, double* y1, const double* const* x2,
+            double* y2, int64_t n, cudaStream_t st);
+void axpys2(int K, const double* dcoef, double sign, const float* const* x1, float* y1, const float* const* x2,
+            float* y2, int64_t n, cudaStream_t st);
+
 // x *= 1/dscal[0] and (if y) y *= 1/dscal[0]; sets *err = 1 when dscal[0] is 0 or not finite.
 void scale_inv2(const double* dscal, double* x, double* y, int64_t n, int* err, cudaStream_t st,
                 const int* active = nullptr);

@@ -479,12 +479,14 @@ struct OrthoT {
   std::vector<DBuf<T>> Sol, Mxx;
   int k = 0;
   int cap = 96;
-  double* d_beta;   // [kMaxDots] projection coefficients
+  double* d_proj;   // [0] |M| after a projection sweep, [1] |M|^2 before it, [2..] projection coefficients
+  double* d_beta;   // = d_proj + 2
   double* d_norm;   // [2]
   double* d_alpha;  // [1]
   bool cancellation = false;
   OrthoT(Ctx& c, const Matrix* A_) : A(A_), N(A_->N) {
-    d_beta = c.scal(kMaxDots);
+    d_proj = c.scal(kMaxDots + 2);
+    d_beta = d_proj + 2;
     d_norm = c.scal(2);
     d_alpha = c.scal(1);
   }
@@ -503,28 +505,37 @@ struct OrthoT {
     dots(c.red, 1, a, a, N, d_norm, 1, c.st);
     return c.get(d_norm);
   }
-  // one classical Gram-Schmidt sweep of (X, M) against the history; returns |M| afterwards
-  double cgs(Ctx& c, T* X, T* M) {
-    for (int i0 = 0; i0 < k; i0 += kMaxDots) {
-      const int kc = std::min(kMaxDots, k - i0);
+  // One classical Gram-Schmidt sweep of (X, M) against the history, launched without a host round trip:
+  // d_proj[0] = |M| after the sweep and, with `self`, d_proj[1] = |M|^2 before it (one more product in the
+  // first multi-dot launch).  History chunks of kMaxDots - 1 vectors; later chunks project the already-updated M
+  // (block MGS).
+  void cgs_launch(Ctx& c, T* X, T* M, bool self) {
+    const int chunk = kMaxDots - 1;
+    for (int i0 = 0; i0 < k; i0 += chunk) {
+      const int kc = std::min(chunk, k - i0);
+      const bool withself = self && i0 == 0;
       const T* a[kMaxDots];
       const T* b[kMaxDots];
-      for (int i = 0; i < kc; ++i) {
-        a[i] = Mxx[i0 + i].p;
-        b[i] = M;
+      int K = 0;
+      if (withself) {
+        a[K] = M;
+        b[K++] = M;
       }
-      dots(c.red, kc, a, b, N, d_beta, 0, c.st);
+      for (int i = 0; i < kc; ++i) {
+        a[K] = Mxx[i0 + i].p;
+        b[K++] = M;
+      }
+      dots(c.red, K, a, b, N, withself ? d_proj + 1 : d_beta, 0, c.st);
       const T* sx[kMaxDots];
       const T* mx[kMaxDots];
       for (int i = 0; i < kc; ++i) {
         sx[i] = Sol[i0 + i].p;
         mx[i] = Mxx[i0 + i].p;
       }
-      // NB: M is updated chunk by chunk, so later chunks project the already-updated M (block MGS)
-      axpys(kc, d_beta, nullptr, -1.0, sx, X, N, c.st);
-      axpys(kc, d_beta, nullptr, -1.0, mx, M, N, c.st);
+      axpys2(kc, d_beta, -1.0, sx, X, mx, M, N, c.st);
     }
-    return norm(c, M);
+    const T* a[1] = {M};
+    dots(c.red, 1, a, a, N, d_proj, 1, c.st);
   }
   void random_restart(Ctx& c, T* X, T* M) {
     fill_random(X, N, c.seed++, c.st);
@@ -533,11 +544,40 @@ struct OrthoT {
     if (nm == 0 || !std::isfinite(nm))
       throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: breakdown with a random vector");
   }
-  // AddSol: Sol[k] holds the new correction; computes Mxx[k] and appends.
+  // AddSol: Sol[k] holds the new correction; computes Mxx[k] = A Sol[k], A-orthonormalises both against the
+  // history and appends.  The normalisation by |M| that the reference applies before the projection
+  // (OrthonormalizationMultigrid.cs:263-337) is folded into the final scaling (the projection is linear), so the
+  // common case costs one SpMV, one multi-dot, one dual multi-axpy, one norm, one scaling and one host round trip.
   void add_sol(Ctx& c) {
     T* X = Sol[k].p;
     T* M = Mxx[k].p;
     spmv(*A, T(1), X, T(0), (const T*)nullptr, M, c.st);
+    if (k > 0) {
+      cgs_launch(c, X, M, true);
+      c.fetch(d_proj, 2);
+      const double nA = c.hscal[d_proj - c.dscal.p];
+      const double nM = std::sqrt(c.hscal[d_proj + 1 - c.dscal.p]);
+      if (!std::isfinite(nM)) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: norm of matrix*solution is NaN/Inf");
+      if (nM > 0) {
+        double rel = nA / nM;
+        if (rel > 1e-5 && rel < 0.5) {
+          cgs_launch(c, X, M, false);
+          rel = c.get(d_proj) / nM;
+        }
+        if (rel > 1e-5) {
+          scale_inv2(d_proj, X, M, N, nullptr, c.st);
+          cancellation = false;
+          ++k;
+          return;
+        }
+        // cancellation: continue in the reference's order from the state it would have (normalised by |M|)
+        axpby(T(1.0 / nM), M, T(0), M, N, c.st);
+        axpby(T(1.0 / nM), X, T(0), X, N, c.st);
+        add_sol_tail(c, X, M, rel);
+        return;
+      }
+      // X == 0: random restart below (M is zero as well)
+    }
     double nM = norm(c, M);
     if (!std::isfinite(nM)) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: norm of matrix*solution is NaN/Inf");
     if (nM == 0) {
@@ -546,11 +586,27 @@ struct OrthoT {
     }
     axpby(T(1.0 / nM), M, T(0), M, N, c.st);
     axpby(T(1.0 / nM), X, T(0), X, N, c.st);
+    add_sol_tail(c, X, M, -1.0);
+  }
+  // the re-orthonormalisation loop of AddSol on normalised (X, M); nn0 >= 0: result of the first sweep
+  void add_sol_tail(Ctx& c, T* X, T* M, double nn0) {
     const int MaxOrtho = 10;
     bool canc = false;
     for (int jj = 0; jj <= MaxOrtho; ++jj) {
-      double nn = (k > 0) ? cgs(c, X, M) : 1.0;
-      if (k > 0 && nn > 1e-5 && nn < 0.5) nn = cgs(c, X, M);
+      double nn;
+      if (jj == 0 && nn0 >= 0) {
+        nn = nn0;
+      } else {
+        nn = 1.0;
+        if (k > 0) {
+          cgs_launch(c, X, M, false);
+          nn = c.get(d_proj);
+          if (nn > 1e-5 && nn < 0.5) {
+            cgs_launch(c, X, M, false);
+            nn = c.get(d_proj);
+          }
+        }
+      }
       if (nn <= 1e-5) {
         canc = true;
         if (jj < MaxOrtho) {
