@@ -23,35 +23,12 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-template <typename T, int KC>
-__global__ void __launch_bounds__(kThreads) dots_kernel(DotArgs<T> args, int K, int64_t n, double* __restrict__ partial,
-                                                        unsigned int* __restrict__ ticket, double* __restrict__ out,
-                                                        int post, const int* __restrict__ active) {
-  if (active != nullptr && *active == 0) return;
-  double acc[KC];
-#pragma unroll
-  for (int k = 0; k < KC; ++k) acc[k] = 0.0;
-  const int64_t stride = (int64_t)gridDim.x * kThreads;
-  int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x;
-  for (; i + stride < n; i += 2 * stride) {
-#pragma unroll
-    for (int k = 0; k < KC; ++k) {
-      if (k < K) {
-        const T* a = args.a[k];
-        const T* b = args.b[k];
-        double a0 = (double)a[i], a1 = (double)a[i + stride];
-        double b0 = (a == b) ? a0 : (double)b[i];
-        double b1 = (a == b) ? a1 : (double)b[i + stride];
-        acc[k] = fma(a0, b0, acc[k]);
-        acc[k] = fma(a1, b1, acc[k]);
-      }
-    }
-  }
-  if (i < n) {
-#pragma unroll
-    for (int k = 0; k < KC; ++k)
-      if (k < K) acc[k] = fma((double)args.a[k][i], (double)args.b[k][i], acc[k]);
-  }
+// Second half of every grid reduction: per-CTA sums of the K accumulators into `partial`, and the last CTA to
+// arrive (threadfence + atomic ticket) adds the partials in a fixed order, so the result does not depend on CTA
+// scheduling.
+template <int KC>
+__device__ __forceinline__ void finish_dots(const double (&acc)[KC], int K, double* __restrict__ partial,
+                                            unsigned int* __restrict__ ticket, double* __restrict__ out, int post) {
   __shared__ double red[kThreads / 32][KC];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -89,6 +66,84 @@ __global__ void __launch_bounds__(kThreads) dots_kernel(DotArgs<T> args, int K, 
   if (threadIdx.x == 0) *ticket = 0u;
 }
 
+template <typename T, int KC>
+__global__ void __launch_bounds__(kThreads) dots_kernel(DotArgs<T> args, int K, int64_t n, double* __restrict__ partial,
+                                                        unsigned int* __restrict__ ticket, double* __restrict__ out,
+                                                        int post, const int* __restrict__ active) {
+  if (active != nullptr && *active == 0) return;
+  double acc[KC];
+#pragma unroll
+  for (int k = 0; k < KC; ++k) acc[k] = 0.0;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  for (; i + stride < n; i += 2 * stride) {
+#pragma unroll
+    for (int k = 0; k < KC; ++k) {
+      if (k < K) {
+        const T* a = args.a[k];
+        const T* b = args.b[k];
+        double a0 = (double)a[i], a1 = (double)a[i + stride];
+        double b0 = (a == b) ? a0 : (double)b[i];
+        double b1 = (a == b) ? a1 : (double)b[i + stride];
+        acc[k] = fma(a0, b0, acc[k]);
+        acc[k] = fma(a1, b1, acc[k]);
+      }
+    }
+  }
+  if (i < n) {
+#pragma unroll
+    for (int k = 0; k < KC; ++k)
+      if (k < K) acc[k] = fma((double)args.a[k][i], (double)args.b[k][i], acc[k]);
+  }
+  finish_dots<KC>(acc, K, partial, ticket, out, post);
+}
+
+// K products against one shared vector b (Gram-Schmidt projections, Arnoldi): b is read once per element and
+// every vector moves in 16-byte loads (all pointers 16-byte aligned; the host checks), so the launch streams
+// (K+1) vectors at HBM rate.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int W = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int W = 2; };
+
+__device__ __forceinline__ double dot16(const float4& a, const float4& b) {
+  return (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+}
+__device__ __forceinline__ double dot16(const double2& a, const double2& b) { return fma(a.x, b.x, a.y * b.y); }
+
+template <typename T, int KC>
+__global__ void __launch_bounds__(kThreads) dots_sharedb_kernel(DotArgs<T> args, int K, int64_t n,
+                                                                double* __restrict__ partial,
+                                                                unsigned int* __restrict__ ticket,
+                                                                double* __restrict__ out, int post,
+                                                                const int* __restrict__ active) {
+  if (active != nullptr && *active == 0) return;
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::W;
+  double acc[KC];
+#pragma unroll
+  for (int k = 0; k < KC; ++k) acc[k] = 0.0;
+  const int64_t nv = n / W;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  const V* bv = reinterpret_cast<const V*>(args.b[0]);
+  for (int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x; j < nv; j += stride) {
+    const V bb = __ldg(bv + j);
+    V aa[KC];
+#pragma unroll
+    for (int k = 0; k < KC; ++k)
+      if (k < K) aa[k] = __ldcs(reinterpret_cast<const V*>(args.a[k]) + j);
+#pragma unroll
+    for (int k = 0; k < KC; ++k)
+      if (k < K) acc[k] += dot16(aa[k], bb);
+  }
+  for (int64_t i = nv * W + (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+    const double b = (double)args.b[0][i];
+#pragma unroll
+    for (int k = 0; k < KC; ++k)
+      if (k < K) acc[k] = fma((double)args.a[k][i], b, acc[k]);
+  }
+  finish_dots<KC>(acc, K, partial, ticket, out, post);
+}
+
 template <typename T>
 void dots_impl(ReduceScratch& s, int K, const T* const* a, const T* const* b, int64_t n, double* out, int post,
                cudaStream_t st, const int* active) {
@@ -100,8 +155,18 @@ void dots_impl(ReduceScratch& s, int K, const T* const* a, const T* const* b, in
     args.b[k] = b[k];
   }
   const int grid = s.grid;
-#define BSGPU_DOTS(KC) \
-  dots_kernel<T, KC><<<grid, kThreads, 0, st>>>(args, K, n, s.partial.p, s.ticket.p, out, post, active)
+  bool shared = true;
+  for (int k = 0; k < K; ++k)
+    shared = shared && b[k] == b[0] && (reinterpret_cast<uintptr_t>(a[k]) % 16 == 0);
+  shared = shared && (reinterpret_cast<uintptr_t>(b[0]) % 16 == 0);
+#define BSGPU_DOTS(KC)                                                                                        \
+  do {                                                                                                        \
+    if (shared)                                                                                               \
+      dots_sharedb_kernel<T, KC><<<grid, kThreads, 0, st>>>(args, K, n, s.partial.p, s.ticket.p, out, post,   \
+                                                            active);                                          \
+    else                                                                                                      \
+      dots_kernel<T, KC><<<grid, kThreads, 0, st>>>(args, K, n, s.partial.p, s.ticket.p, out, post, active);  \
+  } while (0)
   if (K == 1)
     BSGPU_DOTS(1);
   else if (K == 2)
