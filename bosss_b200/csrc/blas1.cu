@@ -27,7 +27,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // arrive (threadfence + atomic ticket) adds the partials in a fixed order, so the result does not depend on CTA
 // scheduling.
 template <int KC>
-__device__ __forceinline__ void finish_dots(const double (&acc)[KC], int K, double* __restrict__ partial,
+__device__ __forceinline__ bool finish_dots(const double (&acc)[KC], int K, double* __restrict__ partial,
                                             unsigned int* __restrict__ ticket, double* __restrict__ out, int post) {
   __shared__ double red[kThreads / 32][KC];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -48,7 +48,7 @@ __device__ __forceinline__ void finish_dots(const double (&acc)[KC], int K, doub
   __shared__ bool last;
   if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
   __syncthreads();
-  if (!last) return;
+  if (!last) return false;
   __threadfence();
   for (int k = 0; k < K; ++k) {
     double s = 0.0;
@@ -64,6 +64,7 @@ __device__ __forceinline__ void finish_dots(const double (&acc)[KC], int K, doub
     }
   }
   if (threadIdx.x == 0) *ticket = 0u;
+  return true;
 }
 
 template <typename T, int KC>
@@ -142,6 +143,77 @@ __global__ void __launch_bounds__(kThreads) dots_sharedb_kernel(DotArgs<T> args,
       if (k < K) acc[k] = fma((double)args.a[k][i], b, acc[k]);
   }
   finish_dots<KC>(acc, K, partial, ticket, out, post);
+}
+
+template <typename T, int NP>
+__global__ void __launch_bounds__(256) pcg_update_kernel(double* __restrict__ s, int* __restrict__ active,
+                                                         T* __restrict__ x, const T* __restrict__ p,
+                                                         const T* __restrict__ q, T* __restrict__ r, T* __restrict__ z,
+                                                         const T* __restrict__ dinv, int64_t nb,
+                                                         double* __restrict__ partial,
+                                                         unsigned int* __restrict__ ticket, int mode, double tol,
+                                                         int max_iter, int min_iter) {
+  if (*active == 0) return;
+  constexpr int BPC = 256 / NP;  // block rows per tile; thread t owns DOF row t % NP of block row t / NP
+  const double alpha = s[0] / s[1];
+  __shared__ T rs[256];
+  double acc[2] = {0.0, 0.0};
+  const int t = threadIdx.x;
+  const int lb = t / NP;
+  const int rr = t - lb * NP;
+  for (int64_t tile = blockIdx.x; tile * BPC < nb; tile += gridDim.x) {
+    const int64_t i = tile * BPC + lb;
+    const bool valid = (lb < BPC) && (i < nb);
+    const int64_t g = i * NP + rr;
+    T rn = T(0);
+    if (valid) {
+      x[g] = (T)((double)x[g] + alpha * (double)p[g]);
+      rn = (T)((double)r[g] - alpha * (double)q[g]);
+      r[g] = rn;
+    }
+    rs[t] = rn;
+    __syncthreads();
+    if (valid) {
+      const T* D = dinv + i * (NP * NP) + rr;
+      const T* rb = rs + lb * NP;
+      T zz = T(0);
+#pragma unroll
+      for (int c = 0; c < NP; ++c) zz = fma(D[c * NP], rb[c], zz);
+      z[g] = zz;
+      acc[0] = fma((double)rn, (double)zz, acc[0]);
+      acc[1] = fma((double)rn, (double)rn, acc[1]);
+    }
+    __syncthreads();
+  }
+  if (finish_dots<2>(acc, 2, partial, ticket, s + 2, 0)) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      pcg_beta_step(s, active, mode, tol, max_iter, min_iter);
+    }
+  }
+}
+
+template <typename T>
+bool pcg_update_impl(ReduceScratch& red, int NP, double* s, int* active, T* x, const T* p, const T* q, T* r, T* z,
+                     const T* dinv, int64_t nb, int mode, double tol, int max_iter, int min_iter, cudaStream_t st) {
+  if (NP != 4 && NP != 6 && NP != 10 && NP != 20) return false;
+  if (nb == 0) return false;
+  if (!red.grid) red.init();
+  const int64_t tiles = (nb + 256 / NP - 1) / (256 / NP);
+  const int grid = (int)std::min<int64_t>(tiles, red.grid);
+#define BSGPU_PCGU(N_)                                                                                          \
+  pcg_update_kernel<T, N_><<<grid, 256, 0, st>>>(s, active, x, p, q, r, z, dinv, nb, red.partial.p, red.ticket.p, \
+                                                 mode, tol, max_iter, min_iter)
+  switch (NP) {
+    case 4: BSGPU_PCGU(4); break;
+    case 6: BSGPU_PCGU(6); break;
+    case 10: BSGPU_PCGU(10); break;
+    default: BSGPU_PCGU(20); break;
+  }
+#undef BSGPU_PCGU
+  BSGPU_CHECK_LAUNCH();
+  return true;
 }
 
 template <typename T>
@@ -384,6 +456,16 @@ void axpys(int K, const double* dcoef, const double* hcoef, double sign, const d
 void axpys(int K, const double* dcoef, const double* hcoef, double sign, const float* const* x, float* y, int64_t n,
            cudaStream_t st, const int* active) {
   axpys_impl<float>(K, dcoef, hcoef, sign, x, y, n, st, active);
+}
+bool pcg_update(ReduceScratch& red, int NP, double* s, int* active, double* x, const double* p, const double* q,
+                double* r, double* z, const double* dinv, int64_t nb, int mode, double tol, int max_iter,
+                int min_iter, cudaStream_t st) {
+  return pcg_update_impl<double>(red, NP, s, active, x, p, q, r, z, dinv, nb, mode, tol, max_iter, min_iter, st);
+}
+bool pcg_update(ReduceScratch& red, int NP, double* s, int* active, float* x, const float* p, const float* q,
+                float* r, float* z, const float* dinv, int64_t nb, int mode, double tol, int max_iter, int min_iter,
+                cudaStream_t st) {
+  return pcg_update_impl<float>(red, NP, s, active, x, p, q, r, z, dinv, nb, mode, tol, max_iter, min_iter, st);
 }
 void axpys2(int K, const double* dcoef, double sign, const double* const* x1, double* y1, const double* const* x2,
             double* y2, int64_t n, cudaStream_t st) {

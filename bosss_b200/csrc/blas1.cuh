@@ -44,6 +44,37 @@ void scale_inv2(const double* dscal, double* x, double* y, int64_t n, int* err, 
 void scale_inv2(const double* dscal, float* x, float* y, int64_t n, int* err, cudaStream_t st,
                 const int* active = nullptr);
 
+// SoftPCG's scalar step after r.z and r.r are known (SoftPCG.cs:113-194 with IterativeSolverConfig's termination):
+// s[0] = r.z (old), s[2] = r.z (new), s[3] = r.r, s[4] = r0.r0, s[5] = iteration count; writes beta to s[6],
+// advances the count and clears *active when the iteration terminates.  Device side, one thread.
+__device__ __forceinline__ void pcg_beta_step(double* s, int* active, int mode, double tol, int max_iter,
+                                              int min_iter) {
+  const double rz_new = s[2], rr = s[3];
+  s[6] = rz_new / s[0];
+  s[0] = rz_new;
+  const double it = s[5] + 1.0;
+  s[5] = it;
+  const double R = sqrt(rr), R0 = sqrt(s[4]);
+  const double eps = 2.2204460492503131e-16 * 1000;
+  bool stop = false;
+  if (it > min_iter) {
+    const bool ok = (mode == 0) ? (R < R0 * tol + tol) : (R < R0 * tol);
+    if (ok || it > max_iter || R < eps || R0 < eps) stop = true;
+  }
+  if (!isfinite(rz_new) || !isfinite(rr)) stop = true;
+  if (stop) *active = 0;
+}
+
+// One fused PCG update for uniform blocks of NP in {4, 6, 10, 20} with a block-Jacobi preconditioner (Dinv
+// column-major per block): alpha = s[0]/s[1]; x += alpha p; r -= alpha q; z = Dinv r; s[2] = r.z, s[3] = r.r;
+// then pcg_beta_step.  No-op when *active == 0.  Returns false (nothing launched) for other block sizes.
+bool pcg_update(ReduceScratch& red, int NP, double* s, int* active, double* x, const double* p, const double* q,
+                double* r, double* z, const double* dinv, int64_t nb, int mode, double tol, int max_iter,
+                int min_iter, cudaStream_t st);
+bool pcg_update(ReduceScratch& red, int NP, double* s, int* active, float* x, const float* p, const float* q,
+                float* r, float* z, const float* dinv, int64_t nb, int mode, double tol, int max_iter, int min_iter,
+                cudaStream_t st);
+
 // y = alpha * x + beta * y  (host scalars)
 void axpby(double alpha, const double* x, double beta, double* y, int64_t n, cudaStream_t st);
 void axpby(float alpha, const float* x, float beta, float* y, int64_t n, cudaStream_t st);

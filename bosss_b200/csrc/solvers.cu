@@ -295,20 +295,7 @@ __global__ void pcg_alpha_kernel(double* s, const int* active) {
 
 __global__ void pcg_beta_kernel(double* s, int* active, int mode, double tol, int max_iter, int min_iter) {
   if (*active == 0) return;
-  const double rz_new = s[2], rr = s[3];
-  s[6] = rz_new / s[0];
-  s[0] = rz_new;
-  const double it = s[5] + 1.0;
-  s[5] = it;
-  const double R = sqrt(rr), R0 = sqrt(s[4]);
-  const double eps = 2.2204460492503131e-16 * 1000;
-  bool stop = false;
-  if (it > min_iter) {
-    const bool ok = (mode == 0) ? (R < R0 * tol + tol) : (R < R0 * tol);
-    if (ok || it > max_iter || R < eps || R0 < eps) stop = true;
-  }
-  if (!isfinite(rz_new) || !isfinite(rr)) stop = true;
-  if (stop) *active = 0;
+  pcg_beta_step(s, active, mode, tol, max_iter, min_iter);
 }
 
 template <typename T>
@@ -394,12 +381,22 @@ struct PCGT : Solver<T> {
     if (!std::isfinite(R0)) throw Error(BSGPU_ERR_ARITHMETIC, "PCG: NaN/Inf in the initial residual");
     if (st0.first) {
       const int grid = elt_grid(N);
+      const bool fused = precond && A->uniform && A->nb > 0 &&
+                         (A->Np == 4 || A->Np == 6 || A->Np == 10 || A->Np == 20);
       const T* px[1] = {p.p};
       const T* qx[1] = {q.p};
       auto batch_kernels = [&]() {
         for (int bi = 0; bi < batch; ++bi) {
           spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, st, active);
           dots(c.red, 1, px, qx, N, s + 1, 0, st, active);
+          if (fused) {
+            // alpha, x and r updates, z = Dinv r, r.z, r.r and the beta / termination step in one launch
+            pcg_update(c.red, A->Np, s, active, X, p.p, q.p, r.p, z.p, dinv.p, A->nb, term.mode, term.tol,
+                       term.max_iter, term.min_iter, st);
+            xpby_kernel<T><<<grid, 256, 0, st>>>(z.p, s + 6, p.p, N, active);
+            BSGPU_CHECK_LAUNCH();
+            continue;
+          }
           pcg_alpha_kernel<<<1, 1, 0, st>>>(s, active);
           BSGPU_CHECK_LAUNCH();
           axpys(1, s + 7, nullptr, 1.0, px, X, N, st, active);
