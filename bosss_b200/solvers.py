@@ -62,7 +62,10 @@ class BlockMsrMatrix:
         nat.check(nat.lib().bsgpu_matrix_create(
             C.byref(h), nb, int(Np), None if nspc is None else nat.ptr(nspc), nat.ptr(row_ptr), nat.ptr(col_idx),
             nat.ptr(values), nat.DEVICE_POINTERS if dev else nat.HOST_POINTERS))
-        return cls(h)
+        M = cls(h)
+        host = (lambda a: a.cpu().numpy()) if dev else (lambda a: a)
+        M._structure = (host(row_ptr), host(col_idx), None if nspc is None else host(nspc))
+        return M
 
     @classmethod
     def from_system(cls, s) -> "BlockMsrMatrix":
@@ -109,6 +112,19 @@ class BlockMsrMatrix:
         h = C.c_void_p()
         nat.check(nat.lib().bsgpu_matrix_restrict(self._h, int(keep), C.byref(h)))
         return BlockMsrMatrix(h)
+
+    def SaveToTextFileSparse(self, path: str) -> int:
+        """Writes the matrix in the text format of BoSSS's SaveToTextFileSparse (IMutuableMatrixEx_Extensions.cs:517);
+        returns the number of non-zero entries.  Available for matrices created with ``from_bsr``."""
+        from .matrixio import save_text_sparse
+        st = getattr(self, "_structure", None)
+        if st is None:
+            raise ValueError("the block structure of this matrix is not known on the host")
+        rp, ci, nspc = st
+        L = (np.ones(self.NoOfBlocks, np.int64) if nspc is None else np.asarray(nspc, np.int64)) * self.Np
+        rows = np.repeat(np.arange(self.NoOfBlocks), np.diff(rp))
+        nvals = int((L[rows] * L[np.asarray(ci)]).sum())
+        return save_text_sparse(path, self.Np, rp, ci, self.read_values(nvals), nspc)
 
     def read_values(self, nvals: Optional[int] = None) -> np.ndarray:
         """All blocks, row-major, in block-CSR order (the layout of ReadBlock).
