@@ -1206,6 +1206,154 @@ struct FlexGMRES : Solver<double> {
 };
 
 // ---------------------------------------------------------------------------------------------------------------
+// SoftGMRES.Solve (SoftGMRES.cs:227-460): restarted GMRES(m) with left preconditioning, r = M^{-1}(b - A x),
+// Arnoldi on M^{-1} A, Givens rotations, x += V y at convergence and at every restart.  As in the reference, the
+// termination test compares the preconditioned residual estimate |s_i| against the unpreconditioned initial
+// residual |b - A x0|.  Gram-Schmidt: classical, one multi-dot and one multi-axpy launch per sweep, two sweeps
+// (the reference uses one modified sweep).  When the iteration limit is reached at the end of a cycle the update of
+// that cycle is applied (the reference leaves x at the start of the cycle).
+// ---------------------------------------------------------------------------------------------------------------
+struct SoftGMRES : Solver<double> {
+  const Matrix* A;
+  int64_t N;
+  int m;
+  Term term;
+  std::unique_ptr<Solver<double>> pc;
+  std::vector<DBuf<double>> V;
+  DBuf<double> Z;
+  double* d_h;     // [2*(m+1)] projections of both sweeps
+  double* d_norm;  // [1]
+  SoftGMRES(Ctx& c, const Matrix* A_, int m_, Term t) : A(A_), N(A_->N), m(m_), term(t) {
+    for (int j = 0; j <= m; ++j) V.emplace_back(std::max<int64_t>(N, 1));
+    Z.alloc(std::max<int64_t>(N, 1));
+    d_h = c.scal(2 * (m + 1));
+    d_norm = c.scal(1);
+  }
+  int nested() const override { return pc ? pc->this_level_iterations + pc->nested() : 0; }
+  double norm(Ctx& c, const double* v) {
+    const double* a[1] = {v};
+    dots(c.red, 1, a, a, N, d_norm, 1, c.st);
+    return c.get(d_norm);
+  }
+  void project(Ctx& c, int j, double* W, int off) {
+    for (int i0 = 0; i0 <= j; i0 += kMaxDots) {
+      const int kc = std::min(kMaxDots, j + 1 - i0);
+      const double* a[kMaxDots];
+      const double* b[kMaxDots];
+      for (int i = 0; i < kc; ++i) {
+        a[i] = V[i0 + i].p;
+        b[i] = W;
+      }
+      dots(c.red, kc, a, b, N, d_h + off + i0, 0, c.st);
+    }
+    std::vector<const double*> vx(j + 1);
+    for (int i = 0; i <= j; ++i) vx[i] = V[i].p;
+    axpys(j + 1, d_h + off, nullptr, -1.0, vx.data(), W, N, c.st);
+  }
+  void precondition(Ctx& c, const double* in, double* out) {
+    if (pc) {
+      fill(0.0, out, N, c.st);
+      pc->solve(c, out, in, true);
+    } else {
+      copy_vec(out, in, N, c.st);
+    }
+  }
+  void solve(Ctx& c, double* X, const double* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), g(m + 1), y(m);
+    this->history.clear();
+    int tot = 0;
+    if (zero)
+      copy_vec(Z.p, B, N, c.st);
+    else
+      spmv(*A, -1.0, X, 1.0, B, Z.p, c.st);
+    const double r0 = norm(c, Z.p);
+    if (!std::isfinite(r0)) throw Error(BSGPU_ERR_ARITHMETIC, "SoftGMRES: residual is NaN/Inf");
+    this->history.push_back(r0);
+    auto st0 = term(0, r0, r0);
+    if (!st0.first) {
+      this->converged = st0.second;
+      this->this_level_iterations = 0;
+      return;
+    }
+    bool first = true;
+    while (true) {
+      if (!first) spmv(*A, -1.0, X, 1.0, B, Z.p, c.st);
+      first = false;
+      precondition(c, Z.p, V[0].p);
+      const double beta = norm(c, V[0].p);
+      if (!std::isfinite(beta)) throw Error(BSGPU_ERR_ARITHMETIC, "SoftGMRES: preconditioned residual is NaN/Inf");
+      if (beta == 0.0) {
+        this->converged = true;
+        break;
+      }
+      axpby(1.0 / beta, V[0].p, 0.0, V[0].p, N, c.st);
+      std::fill(g.begin(), g.end(), 0.0);
+      g[0] = beta;
+      int j;
+      bool stop = false;
+      double err = beta;
+      for (j = 0; j < m; ++j) {
+        spmv(*A, 1.0, V[j].p, 0.0, (const double*)nullptr, Z.p, c.st);
+        double* W = V[j + 1].p;
+        precondition(c, Z.p, W);
+        project(c, j, W, 0);
+        project(c, j, W, m + 1);
+        const double* a[1] = {W};
+        dots(c.red, 1, a, a, N, d_norm, 1, c.st);
+        c.fetch(d_h, 2 * (m + 1) + 1);
+        const double* hh = c.hscal + (d_h - c.dscal.p);
+        const double wn = hh[2 * (m + 1)];
+        if (!std::isfinite(wn)) throw Error(BSGPU_ERR_ARITHMETIC, "SoftGMRES: Arnoldi vector is NaN/Inf");
+        for (int i = 0; i <= j; ++i) H[i * m + j] = hh[i] + hh[m + 1 + i];
+        H[(j + 1) * m + j] = wn;
+        if (wn > 0) axpby(1.0 / wn, W, 0.0, W, N, c.st);
+        for (int i = 0; i < j; ++i) {
+          const double a0 = H[i * m + j], b0 = H[(i + 1) * m + j];
+          H[i * m + j] = cs[i] * a0 + sn[i] * b0;
+          H[(i + 1) * m + j] = -sn[i] * a0 + cs[i] * b0;
+        }
+        const double a0 = H[j * m + j], b0 = H[(j + 1) * m + j];
+        const double den = std::hypot(a0, b0);
+        cs[j] = a0 / den;
+        sn[j] = b0 / den;
+        H[j * m + j] = den;
+        H[(j + 1) * m + j] = 0.0;
+        g[j + 1] = -sn[j] * g[j];
+        g[j] = cs[j] * g[j];
+        err = std::fabs(g[j + 1]);
+        this->history.push_back(err);
+        auto st1 = term(tot, r0, err);
+        ++tot;
+        if (!st1.first || wn == 0.0) {
+          stop = true;
+          this->converged = st1.second || wn == 0.0;
+          ++j;
+          break;
+        }
+      }
+      const int kk = j;
+      for (int i = kk - 1; i >= 0; --i) {
+        double s = g[i];
+        for (int q = i + 1; q < kk; ++q) s -= H[i * m + q] * y[q];
+        y[i] = s / H[i * m + i];
+      }
+      std::vector<const double*> vx(kk);
+      for (int i = 0; i < kk; ++i) vx[i] = V[i].p;
+      axpys(kk, nullptr, y.data(), 1.0, vx.data(), X, N, c.st);
+      if (stop) break;
+      auto st2 = term(tot, r0, err);
+      if (!st2.first) {
+        this->converged = st2.second;
+        break;
+      }
+    }
+    this->this_level_iterations = tot;
+    if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += tot;
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
 // tree construction (PmgConfig.CreateInstanceImpl__Kummer, PmgConfig.cs:80-245, with UseILU = false)
 // ---------------------------------------------------------------------------------------------------------------
 template <typename T>
@@ -1419,7 +1567,8 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
   top.tol = cfg.tol;
   top.max_iter = cfg.max_iter;
   top.min_iter = cfg.min_iter;
-  if (cfg.solver != BSGPU_SOLVER_SOFTPCG && cfg.solver != BSGPU_SOLVER_BLOCKJACOBI) {
+  if (cfg.solver != BSGPU_SOLVER_SOFTPCG && cfg.solver != BSGPU_SOLVER_BLOCKJACOBI &&
+      !(cfg.solver == BSGPU_SOLVER_SOFTGMRES && cfg.n_levels <= 1)) {
     require(cfg.level_keep[0] == A->Np, "level_keep[0] must equal Np");
     for (int l = 1; l < cfg.n_levels; ++l)
       require(cfg.level_keep[l] >= 1 && cfg.level_keep[l] < cfg.level_keep[l - 1], "level_keep must decrease");
@@ -1473,6 +1622,28 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
         f->pc2 = std::make_unique<LearnedPrecondT<double>>(*t->ctx, t->net.get());
         f->pc2->trace = t->ctx->trace_id("LearnedStage");
         f->stall = cfg.learned_stall > 0 ? cfg.learned_stall : 0.99;
+      }
+      t->top = std::move(f);
+      break;
+    }
+    case BSGPU_SOLVER_SOFTGMRES: {
+      require(cfg.max_krylov >= 1 && cfg.max_krylov <= 256, "max_krylov must be in 1..256");
+      Term one;
+      one.mode = 2;
+      one.max_iter = 1;
+      auto f = std::make_unique<SoftGMRES>(*t->ctx, A, cfg.max_krylov, top);
+      f->trace = t->ctx->trace_id("SoftGMRES");
+      if (cfg.n_levels >= 1 && cfg.level_keep[0] == A->Np && cfg.n_levels > 1) {
+        if (mixed) {
+          auto ad = std::make_unique<MixedAdapter>(A->N);
+          ad->inner = build_level<float>(*t, A, level_matrix<float>(*t, A), 0, one);
+          f->pc = std::move(ad);
+        } else {
+          f->pc = build_level<double>(*t, A, A, 0, one);
+        }
+      } else if (cfg.bj_iters >= 0) {
+        require(!mixed, "mixed precision is available for the p-multigrid preconditioner", BSGPU_ERR_UNSUPPORTED);
+        f->pc = make_smoother<double>(*t->ctx, A, A, cfg.smoother, cfg, "");
       }
       t->top = std::move(f);
       break;

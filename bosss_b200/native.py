@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libbsgpu.so")
 OK, ERR_ARGUMENT, ERR_CUDA, ERR_ARITHMETIC, ERR_NOMEM, ERR_UNSUPPORTED, ERR_TIMEOUT = range(7)
 HOST_POINTERS, DEVICE_POINTERS = 0, 1
 COB_EYE, COB_DIAG_BLOCK_EQUILIB = 0, 1
-SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI = 0, 1, 2, 3
+SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI, SOLVER_SOFTGMRES = 0, 1, 2, 3, 4
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1

@@ -332,6 +332,42 @@ class FGMRESConfig(IterativeSolverConfig):
 
 
 @dataclass
+class SoftGMRESConfig(IterativeSolverConfig):
+    """SoftGMRES (SoftGMRES.cs:75,227-460): restarted GMRES(MaxKrylovDim) with left preconditioning.
+
+    ``Precond``: a ``PmgConfig`` (one p-multigrid V-cycle; ``MixedPrecision`` runs it in FP32), one of the block
+    smoothers "blockjacobi", "schwarz", "ilu" (``BlockJacobiIterations`` sweeps for block Jacobi / Schwarz), or
+    None.  The termination test compares the preconditioned residual estimate with the unpreconditioned initial
+    residual, as the reference does.
+    """
+    MaxKrylovDim: int = 80
+    Precond: object = None
+    MixedPrecision: bool = False
+    BlockJacobiIterations: int = 1
+
+    def _config(self):
+        c = self._base()
+        c.solver = nat.SOLVER_SOFTGMRES
+        c.max_krylov = self.MaxKrylovDim
+        if isinstance(self.Precond, PmgConfig):
+            self.Precond._fill(c)
+            c.precision = nat.PRECISION_MIXED if self.MixedPrecision else nat.PRECISION_FP64
+            return c
+        if self.MixedPrecision:
+            raise ValueError("MixedPrecision needs a PmgConfig preconditioner")
+        c.n_levels = 1
+        kinds = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU}
+        if self.Precond is None:
+            c.bj_iters = -1
+        elif self.Precond in kinds:
+            c.smoother = kinds[self.Precond]
+            c.bj_iters = self.BlockJacobiIterations
+        else:
+            raise ValueError(f"Precond must be a PmgConfig, one of {sorted(kinds)} or None")
+        return c
+
+
+@dataclass
 class SoftPCGConfig(IterativeSolverConfig):
     """SoftPCG (SoftPCG.cs:37) preconditioned by the inverse block diagonal (``BlockJacobiPrecond``)."""
     BlockJacobiPrecond: bool = True
