@@ -1631,20 +1631,17 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
       Term one;
       one.mode = 2;
       one.max_iter = 1;
+      // left preconditioning needs the same operator M^{-1} in every application: a block smoother, not the
+      // p-multigrid V-cycle (its ORTHOMIN minimisation and capped coarse solves vary between calls; FlexGMRES
+      // is the Krylov method for it)
+      require(cfg.n_levels <= 1, "SoftGMRES takes a block-smoother preconditioner (n_levels <= 1); use "
+              "FlexGMRES for the p-multigrid V-cycle", BSGPU_ERR_UNSUPPORTED);
+      require(!mixed, "mixed precision is available for the FlexGMRES p-multigrid preconditioner",
+              BSGPU_ERR_UNSUPPORTED);
+      (void)one;
       auto f = std::make_unique<SoftGMRES>(*t->ctx, A, cfg.max_krylov, top);
       f->trace = t->ctx->trace_id("SoftGMRES");
-      if (cfg.n_levels >= 1 && cfg.level_keep[0] == A->Np && cfg.n_levels > 1) {
-        if (mixed) {
-          auto ad = std::make_unique<MixedAdapter>(A->N);
-          ad->inner = build_level<float>(*t, A, level_matrix<float>(*t, A), 0, one);
-          f->pc = std::move(ad);
-        } else {
-          f->pc = build_level<double>(*t, A, A, 0, one);
-        }
-      } else if (cfg.bj_iters >= 0) {
-        require(!mixed, "mixed precision is available for the p-multigrid preconditioner", BSGPU_ERR_UNSUPPORTED);
-        f->pc = make_smoother<double>(*t->ctx, A, A, cfg.smoother, cfg, "");
-      }
+      if (cfg.bj_iters >= 0) f->pc = make_smoother<double>(*t->ctx, A, A, cfg.smoother, cfg, "");
       t->top = std::move(f);
       break;
     }

@@ -335,14 +335,14 @@ class FGMRESConfig(IterativeSolverConfig):
 class SoftGMRESConfig(IterativeSolverConfig):
     """SoftGMRES (SoftGMRES.cs:75,227-460): restarted GMRES(MaxKrylovDim) with left preconditioning.
 
-    ``Precond``: a ``PmgConfig`` (one p-multigrid V-cycle; ``MixedPrecision`` runs it in FP32), one of the block
-    smoothers "blockjacobi", "schwarz", "ilu" (``BlockJacobiIterations`` sweeps for block Jacobi / Schwarz), or
-    None.  The termination test compares the preconditioned residual estimate with the unpreconditioned initial
+    ``Precond``: one of the block smoothers "blockjacobi", "schwarz", "ilu" (``BlockJacobiIterations`` sweeps for
+    block Jacobi / Schwarz), or None.  Left preconditioning needs the same M^{-1} in every application, so the
+    p-multigrid V-cycle (which varies between calls) belongs in ``FGMRESConfig``; a ``PmgConfig`` is rejected.
+    The termination test compares the preconditioned residual estimate with the unpreconditioned initial
     residual, as the reference does.
     """
     MaxKrylovDim: int = 80
     Precond: object = None
-    MixedPrecision: bool = False
     BlockJacobiIterations: int = 1
 
     def _config(self):
@@ -350,11 +350,7 @@ class SoftGMRESConfig(IterativeSolverConfig):
         c.solver = nat.SOLVER_SOFTGMRES
         c.max_krylov = self.MaxKrylovDim
         if isinstance(self.Precond, PmgConfig):
-            self.Precond._fill(c)
-            c.precision = nat.PRECISION_MIXED if self.MixedPrecision else nat.PRECISION_FP64
-            return c
-        if self.MixedPrecision:
-            raise ValueError("MixedPrecision needs a PmgConfig preconditioner")
+            raise ValueError("SoftGMRES takes a block-smoother preconditioner; use FGMRESConfig for p-multigrid")
         c.n_levels = 1
         kinds = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU}
         if self.Precond is None:

@@ -124,8 +124,8 @@ enum {
   BSGPU_SOLVER_FGMRES_PMG = 1,  /* FlexGMRES.cs:144 (Saad FGMRES(m)) preconditioned by one p-MG V-cycle     */
   BSGPU_SOLVER_ORTHOMG = 2,     /* PmgConfig.cs:80 OrthonormalizationMultigrid p-multigrid as the solver    */
   BSGPU_SOLVER_BLOCKJACOBI = 3, /* the smoother cfg.smoother selects (BlockJacobi.cs:35, Schwarz.cs:56) alone */
-  BSGPU_SOLVER_SOFTGMRES = 4    /* SoftGMRES.cs:227 left-preconditioned GMRES(m): p-MG V-cycle (n_levels > 1) or
-                                   the cfg.smoother block preconditioner (n_levels <= 1; none if bj_iters < 0) */
+  BSGPU_SOLVER_SOFTGMRES = 4    /* SoftGMRES.cs:227 left-preconditioned GMRES(m) with the cfg.smoother block
+                                   preconditioner (n_levels <= 1; none if bj_iters < 0) */
 };
 enum { BSGPU_TERM_DEFAULT = 0 /* R < R0*tol + tol */, BSGPU_TERM_RELATIVE = 1 /* R < R0*tol */ };
 /* coarsest-level solver: dense inverse (p = 0, <= 4096 unknowns), block-Jacobi PCG, or PCG preconditioned by a

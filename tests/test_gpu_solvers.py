@@ -266,18 +266,23 @@ def test_learned_stage_needs_cell_graph(cuda):
         FGMRESConfig(Preconditioners=[PmgConfig(DegreeHierarchy=(10, 4))], Learned="fgmres").CreateInstance(op)
 
 
-@pytest.mark.parametrize("precond", [None, "blockjacobi", "ilu", "pmg", "pmg-mixed"])
+@pytest.mark.parametrize("precond", [None, "blockjacobi", "ilu"])
 def test_softgmres(cuda, precond):
     """SoftGMRES (left-preconditioned restarted GMRES) against the direct solve."""
     from bosss_b200.solvers import SoftGMRESConfig
     s = A.poisson_3d(5, 2)
     op = MultigridOperator(BlockMsrMatrix.from_system(s))
-    pc = PmgConfig(DegreeHierarchy=(10, 4), CoarseTolerance=1e-2) if precond and precond.startswith("pmg") else precond
     slv = SoftGMRESConfig(ConvergenceCriterion=1e-13, termination="relative", MaxKrylovDim=40,
-                          MaxSolverIterations=3000, Precond=pc,
-                          MixedPrecision=precond == "pmg-mixed").CreateInstance(op)
+                          MaxSolverIterations=3000, Precond=precond).CreateInstance(op)
     x = np.zeros(s.N)
     slv.Solve(x, s.rhs)
     xd = _direct(s)
     assert slv.Converged
     assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+def test_softgmres_rejects_pmg(cuda):
+    from bosss_b200.solvers import SoftGMRESConfig
+    op = MultigridOperator(BlockMsrMatrix.from_system(A.poisson_3d(3, 2)))
+    with pytest.raises(ValueError):
+        SoftGMRESConfig(Precond=PmgConfig(DegreeHierarchy=(10, 4))).CreateInstance(op)
