@@ -9,7 +9,7 @@ the volumes and on the faces (diffusivity mu_s), plus SIP coupling of the two sp
     a_G(u, v) = int_G ( -{mu du/dn}[v] - {mu dv/dn}[u] + eta_G [u][v] ),  [u] = u_A - u_B,  n from A to B,
 with eta_G = penalty * cj * max(mu_A, mu_B) (the "max |mu|" SIP variant).
 
-Simplifications of the cut-cell machinery (the solver path, not the discretisation, is what this build
+Simplifications of the cut-cell machinery (the solver path, not the discretisation, is what this library
 accelerates): volume integrals in cut cells use a subdivision rule (sub^3 sub-boxes, Gauss points classified by
 the sign of phi); face integrals touching cut cells use sub^2 sub-squares likewise; the interface integral uses a
 dense Fibonacci point set on the sphere with exact normals; species parts below `frac_min` of a cell are dropped

@@ -40,7 +40,7 @@ enum {
   BSGPU_ERR_CUDA = 2,          /* CUDA runtime error (see bsgpu_last_error)                                */
   BSGPU_ERR_ARITHMETIC = 3,    /* ArithmeticException: NaN/Inf, zero pivot, residual increase, breakdown    */
   BSGPU_ERR_NOMEM = 4,         /* device allocation failed                                                 */
-  BSGPU_ERR_UNSUPPORTED = 5,   /* feature/size not supported by this build                                 */
+  BSGPU_ERR_UNSUPPORTED = 5,   /* feature/size not supported by this library                               */
   BSGPU_ERR_TIMEOUT = 6        /* a bounded device-side wait gave up                                       */
 };
 
