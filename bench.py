@@ -195,7 +195,7 @@ def run_reference(args):
     from bosss_b200 import assembly as A
     threads = os.cpu_count() or 1
     s = A.poisson_3d(args.n, args.p, seed=args.seed)
-    iters = _reference_iterations(args)
+    iters, iters_src = _reference_iterations(args)
     ref = CpuReference(s, threads)
     samples = []
     for i in range(args.warmup + args.steps):
@@ -211,8 +211,8 @@ def run_reference(args):
         "config": {"workload": WORKLOAD, "l2": "inputs larger than L2 (5.8 GB matrix)"},
         "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
                          "sample": f"per step: one SpMV and an FGMRES solve stopped at its first test (2 outer "
-                                   f"iterations = 2 V-cycles), per-iteration time x {iters} iterations (the CPU "
-                                   f"restatement's own count on this system); SpMV {samples[-1]['spmv_gbs']:.1f} GB/s"},
+                                   f"iterations = 2 V-cycles), per-iteration time x {iters} iterations ({iters_src}); "
+                                   f"SpMV {samples[-1]['spmv_gbs']:.1f} GB/s"},
         "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "detail": samples[-1],
     }
@@ -220,11 +220,13 @@ def run_reference(args):
 
 
 def _reference_iterations(args):
-    """Outer iteration count of the oracle on this system (committed with the script that produced it)."""
+    """Outer iteration count of the CPU restatement on this system and where it comes from: the committed full
+    solve for the default system (tests/golden/c2_oracle_solve.json, with the script that produced it), else the
+    same count assumed."""
     path = os.path.join(ROOT, "tests", "golden", "c2_oracle_solve.json")
     if os.path.exists(path) and args.n == 64 and args.p == 3 and args.seed == 0:
-        return int(json.load(open(path))["iterations"])
-    return 9
+        return int(json.load(open(path))["iterations"]), "the CPU restatement's own count on this system"
+    return 9, "assumed equal to the default system's count"
 
 
 # ----------------------------------------------------------------------------------------------------------------
