@@ -344,6 +344,7 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->learned_hidden = 64;
     cfg->learned_stall = 0.99;
     cfg->ortho_max_krylov = 96;
+    cfg->recalc_resi_period = 1;
   });
 }
 

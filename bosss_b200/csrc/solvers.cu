@@ -487,6 +487,8 @@ struct OrthoT {
     d_norm = c.scal(2);
     d_alpha = c.scal(1);
   }
+  int recalc_period = 1;        // RecalcResiPeriod (OrthonormalizationMultigrid.cs:211)
+  bool used_more_cycles = false;  // m_UsedMoreThanOneOrthoCycle: a re-orthonormalisation happened
   void clear() { k = 0; }
   bool full() const { return k >= cap; }
   T* next_sol(Ctx& c) {
@@ -629,9 +631,13 @@ struct OrthoT {
       }
     }
     cancellation = canc;
+    if (canc) used_more_cycles = true;
     ++k;
   }
   // MinimizeResidual: X += alpha*Sol[k-1], alpha = <Mxx[k-1], Res0>; Res = B - A*X; returns |Res|.
+  // With RecalcResiPeriod > 1 the residual is updated as Res -= alpha Mxx[k-1] and recomputed from scratch only
+  // when the history length is a multiple of the period or after a re-orthonormalisation
+  // (OrthonormalizationMultigrid.cs:171-190).
   double minimize(Ctx& c, T* X, const T* B, const T* Res0, T* Res, double oldN) {
     const int i = k - 1;
     const T* a[1] = {Mxx[i].p};
@@ -639,7 +645,12 @@ struct OrthoT {
     dots(c.red, 1, a, b, N, d_alpha, 0, c.st);
     const T* sx[1] = {Sol[i].p};
     axpys(1, d_alpha, nullptr, 1.0, sx, X, N, c.st);
-    spmv(*A, T(-1), X, T(1), B, Res, c.st);
+    if (recalc_period <= 1 || used_more_cycles || k % recalc_period == 0) {
+      spmv(*A, T(-1), X, T(1), B, Res, c.st);
+    } else {
+      const T* mx[1] = {Mxx[i].p};
+      axpys(1, d_alpha, nullptr, -1.0, mx, Res, N, c.st);
+    }
     const double rn = norm(c, Res);
     if (!std::isfinite(rn)) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: residual is NaN/Inf");
     const double tol = std::max(std::max(rn, oldN) * 0.2, 1.0e-7);
@@ -1397,6 +1408,7 @@ std::unique_ptr<Solver<T>> build_hlevel(Tree& t, const Matrix* A64, const Matrix
   ht.max_iter = std::max(1, cfg.h_cycle);
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
+  omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = cfg.h_sweeps;
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -1468,6 +1480,7 @@ std::unique_ptr<Solver<T>> build_hmg_level(Tree& t, const HmgHierarchy* H, const
   }
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
+  omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = std::max(1, cfg.h_sweeps);
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -1531,6 +1544,7 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   const std::string lv = "L" + std::to_string(level);
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
+  omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
   omg->trace = c.trace_id(lv + ".OrthoMG");
   if (level == 0 && t.net && (cfg.learned & BSGPU_LEARNED_PRESMOOTH)) {
     omg->pre = std::make_unique<LearnedPrecondT<T>>(c, t.net.get());

@@ -44,7 +44,7 @@ class SolverConfig(C.Structure):
                 ("precision", C.c_int32), ("h_levels", C.c_int32), ("h_sweeps", C.c_int32), ("h_cycle", C.c_int32),
                 ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
                 ("learned", C.c_int32), ("learned_hidden", C.c_int32), ("learned_stall", C.c_double),
-                ("ortho_max_krylov", C.c_int32), ("reserved", C.c_int32 * 5)]
+                ("ortho_max_krylov", C.c_int32), ("recalc_resi_period", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class SolveStats(C.Structure):

@@ -261,6 +261,7 @@ class PmgConfig(IterativeSolverConfig):
     Smoother: str = "blockjacobi"
     HSmoother: str = "blockjacobi"
     OrthoMaxKrylovDim: int = 96     # OrthonormalizationMultigrid.Config.MaxKrylovDim: history length per level
+    RecalcResiPeriod: int = 1       # OrthonormalizationMultigrid.RecalcResiPeriod: full residual every n updates
     UseILU: bool = False
 
     def _fill(self, c):
@@ -291,6 +292,9 @@ class PmgConfig(IterativeSolverConfig):
         if self.OrthoMaxKrylovDim < 2:
             raise ValueError("OrthoMaxKrylovDim must be at least 2")
         c.ortho_max_krylov = self.OrthoMaxKrylovDim
+        if self.RecalcResiPeriod < 1:
+            raise ValueError("RecalcResiPeriod must be at least 1")
+        c.recalc_resi_period = self.RecalcResiPeriod
 
     def _config(self):
         c = self._base()

@@ -179,7 +179,9 @@ typedef struct {
   int32_t ortho_max_krylov; /* OrthoMG history length (OrthonormalizationMultigrid.Config.MaxKrylovDim,
                                OrthonormalizationMultigrid.cs:486); when full, the minimisation restarts from
                                the current iterate (default 96)                                  */
-  int32_t reserved[5];
+  int32_t recalc_resi_period; /* OrthoMG RecalcResiPeriod (OrthonormalizationMultigrid.cs:211): the residual is
+                                 recomputed from scratch every this many history entries, else updated (default 1) */
+  int32_t reserved[4];
 } bsgpu_solver_config;
 
 typedef struct {

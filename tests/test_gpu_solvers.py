@@ -286,3 +286,18 @@ def test_softgmres_rejects_pmg(cuda):
     op = MultigridOperator(BlockMsrMatrix.from_system(A.poisson_3d(3, 2)))
     with pytest.raises(ValueError):
         SoftGMRESConfig(Precond=PmgConfig(DegreeHierarchy=(10, 4))).CreateInstance(op)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_recalc_resi_period(cuda, mixed):
+    """RecalcResiPeriod > 1: the OrthoMG residual is updated and recomputed every 40 history entries."""
+    s = A.poisson_3d(8, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = PmgConfig(DegreeHierarchy=(20, 10, 4), CoarseTolerance=1e-1, CoarseMaxIterations=60, RecalcResiPeriod=40)
+    slv = FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative", Preconditioners=[pmg],
+                       MixedPrecision=mixed).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    xd = _direct(s)
+    assert slv.Converged
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
