@@ -32,9 +32,11 @@ METRIC = "time-to-1e-10 residual & iters: learned+mixed vs plain FP64 GPU; SpMV 
 WORKLOAD = "SIP DG Poisson 3-D 64^3 hex, p=3 (Np=20, 5.24M DOF), FlexGMRES(30) + 3-level p-MG (3->2->1), BJ smoothing"
 TOL = 1e-10
 # p-multigrid settings shared by every path (PmgConfig.cs:80-245 with UseILU = false; the coarsest p = 1 level,
-# a direct solve in the reference, is block-Jacobi PCG to 0.1 reduction, at most 60 iterations)
+# a direct solve in the reference, is block-Jacobi PCG to 0.1 reduction, at most 60 iterations; the OrthoMG
+# residual is recomputed from scratch every 40 updates, the reference's RecalcResiPeriod parameter,
+# OrthonormalizationMultigrid.cs:179-211)
 SOLVER_PARAMS = dict(NoOfPostSmootherSweeps=10, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.1,
-                     CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100)
+                     CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, RecalcResiPeriod=40)
 
 
 def parse():
@@ -166,7 +168,8 @@ class CpuReference:
                              coarse_kind=O.COARSE_PCG, coarse_tol=SOLVER_PARAMS["CoarseTolerance"],
                              coarse_max_iter=SOLVER_PARAMS["CoarseMaxIterations"],
                              sub_reduction=SOLVER_PARAMS["SubLevelReduction"],
-                             sub_max_iter=SOLVER_PARAMS["SubLevelMaxIterations"], max_iter=1, min_iter=0)
+                             sub_max_iter=SOLVER_PARAMS["SubLevelMaxIterations"], max_iter=1, min_iter=0,
+                             recalc_resi_period=SOLVER_PARAMS["RecalcResiPeriod"])
         t0 = time.perf_counter()
         self.solver = O.PersistentSolver(self.Bt, cfg)
         self.t_setup = time.perf_counter() - t0
@@ -436,7 +439,8 @@ XDGBATCH = ("independent XDG sphere problems, edge in {16,24,32,40,48}, p=2, rad
 # p-multigrid settings of these workloads: FP32 Schwarz smoothing (4 post-sweeps) for the fast path, the plain
 # FP64 path as in the default workload (block Jacobi, 10 post-sweeps)
 PMG_SCHWARZ = dict(NoOfPostSmootherSweeps=4, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.1,
-                   CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, Smoother="schwarz")
+                   CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, Smoother="schwarz",
+                   RecalcResiPeriod=40)
 PMG_BJ = dict(SOLVER_PARAMS, Smoother="blockjacobi")
 
 

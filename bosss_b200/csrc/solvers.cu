@@ -488,7 +488,7 @@ struct OrthoT {
     d_alpha = c.scal(1);
   }
   int recalc_period = 1;        // RecalcResiPeriod (OrthonormalizationMultigrid.cs:211)
-  bool used_more_cycles = false;  // m_UsedMoreThanOneOrthoCycle: a re-orthonormalisation happened
+  bool used_more_cycles = false;  // m_UsedMoreThanOneOrthoCycle: the last AddSol needed more than one sweep
   void clear() { k = 0; }
   bool full() const { return k >= cap; }
   T* next_sol(Ctx& c) {
@@ -566,6 +566,7 @@ struct OrthoT {
         if (rel > 1e-5) {
           scale_inv2(d_proj, X, M, N, nullptr, c.st);
           cancellation = false;
+          used_more_cycles = false;
           ++k;
           return;
         }
@@ -631,7 +632,7 @@ struct OrthoT {
       }
     }
     cancellation = canc;
-    if (canc) used_more_cycles = true;
+    used_more_cycles = canc;
     ++k;
   }
   // MinimizeResidual: X += alpha*Sol[k-1], alpha = <Mxx[k-1], Res0>; Res = B - A*X; returns |Res|.

@@ -488,17 +488,21 @@ struct Ortho {
     Sol.push_back(std::move(X));
     Mxx.push_back(std::move(M));
   }
-  // MinimizeResidual (:149-209) with RecalcResiPeriod = 1.
+  // MinimizeResidual (:149-209): the residual is updated, and recomputed from scratch when the history length is
+  // a multiple of RecalcResiPeriod or the last AddSol needed more than one sweep (:179-190).
+  int recalc_period = 1;
   double minimize(Vec& X, Vec& Sol0, const Vec& Res0, Vec& Res) {
     double oldN = nrm2(Res);
     size_t i = Sol.size() - 1;
     double alpha = dot(Mxx[i], Res0);
     axpy(alpha, Sol[i], X);
     axpy(-alpha, Mxx[i], Res);
-    Res = Res0;
-    axpy(-1.0, X, Sol0);
-    spmv(*A, 1.0, Sol0.data(), 1.0, Res.data());
-    axpy(1.0, X, Sol0);
+    if (recalc_period <= 1 || more_than_one || Sol.size() % (size_t)recalc_period == 0) {
+      Res = Res0;
+      axpy(-1.0, X, Sol0);
+      spmv(*A, 1.0, Sol0.data(), 1.0, Res.data());
+      axpy(1.0, X, Sol0);
+    }
     double N = nrm2(Res);
     double tol = std::max(std::max(N, oldN) * 0.2, 1.0e-7);
     if (N > oldN + tol) throw std::runtime_error("Ortho: residual increase");
@@ -749,6 +753,7 @@ Solver* build_level(const Mat* A, const or_solver_cfg* c, int level, std::vector
     t.max_iter = c->sub_max_iter;
   }
   auto* omg = new OrthoMG(A, t);
+  omg->ortho.recalc_period = c->recalc_resi_period;
   omg->sweeps = c->post_sweeps;
   omg->post = new BlockJacobi(A, c->bj_iters, c->bj_omega);
   auto* gr = new GridAndDegRestriction(A, c->level_keep[level + 1]);

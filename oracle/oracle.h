@@ -34,6 +34,7 @@ typedef struct {
   int32_t sub_max_iter;
   double sub_reduction;
   int32_t reference_fgmres_defect;
+  int32_t recalc_resi_period; /* OrthoMG RecalcResiPeriod (OrthonormalizationMultigrid.cs:211); <= 1: every update */
 } or_solver_cfg;
 
 typedef struct {

@@ -32,7 +32,7 @@ class _Cfg(C.Structure):
                 ("level_keep", C.c_int32 * 8), ("post_sweeps", C.c_int32), ("bj_iters", C.c_int32),
                 ("bj_omega", C.c_double), ("coarse_kind", C.c_int32), ("coarse_tol", C.c_double),
                 ("coarse_max_iter", C.c_int32), ("sub_max_iter", C.c_int32), ("sub_reduction", C.c_double),
-                ("reference_fgmres_defect", C.c_int32)]
+                ("reference_fgmres_defect", C.c_int32), ("recalc_resi_period", C.c_int32)]
 
 
 class _Stats(C.Structure):
@@ -206,6 +206,7 @@ class SolverConfig:
     sub_max_iter: int = 100
     sub_reduction: float = 0.1
     reference_fgmres_defect: bool = False
+    recalc_resi_period: int = 1
 
     def _c(self) -> _Cfg:
         c = _Cfg()
@@ -218,6 +219,7 @@ class SolverConfig:
         c.coarse_kind, c.coarse_tol, c.coarse_max_iter = self.coarse_kind, self.coarse_tol, self.coarse_max_iter
         c.sub_max_iter, c.sub_reduction = self.sub_max_iter, self.sub_reduction
         c.reference_fgmres_defect = int(bool(self.reference_fgmres_defect))
+        c.recalc_resi_period = int(self.recalc_resi_period)
         return c
 
 

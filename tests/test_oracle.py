@@ -190,3 +190,15 @@ def test_ilu0_reproduces_the_matrix_on_its_pattern(ordered):
     b = np.random.default_rng(1).standard_normal(N)
     x = O.ilu0_solve(Bo, F.reshape(-1), b, order if ordered else None)
     assert np.abs(L @ U @ x - b).max() <= 1e-10 * np.abs(b).max()
+
+
+def test_recalc_resi_period_keeps_the_solution():
+    """RecalcResiPeriod > 1 (OrthonormalizationMultigrid.cs:179-211) changes only how the OrthoMG residual is kept."""
+    s = A.poisson_3d(4, 2, seed=2)
+    xd = O.direct_solve(s)
+    for period in (1, 5):
+        cfg = O.SolverConfig(solver=O.FGMRES_PMG, tol=1e-12, level_keep=(10, 4), recalc_resi_period=period,
+                             coarse_tol=1e-2)
+        r = O.solve(O.Bsr.of(s), s.rhs, cfg)
+        assert r.converged
+        assert np.linalg.norm(r.x - xd) <= 1e-9 * np.linalg.norm(xd)
