@@ -150,3 +150,16 @@ def greedy_colour_order(row_ptr, col_idx) -> np.ndarray:
             c += 1
         col[i] = c
     return np.concatenate([np.nonzero(col == c)[0] for c in range(col.max() + 1)]).astype(np.int32)
+
+
+def dense_block_system(nb: int, Np: int, seed: int = 0) -> VarBsr:
+    """Symmetric positive definite system whose block graph is complete (every block row couples to every cell)."""
+    rng = np.random.default_rng(seed)
+    N = nb * Np
+    G = rng.standard_normal((N, N))
+    M = G @ G.T + N * np.eye(N)
+    row_ptr = np.arange(nb + 1, dtype=np.int64) * nb
+    col_idx = np.tile(np.arange(nb, dtype=np.int32), nb)
+    values = np.concatenate([M[i * Np:(i + 1) * Np, j * Np:(j + 1) * Np].ravel() for i in range(nb) for j in range(nb)])
+    return VarBsr(Np=Np, row_ptr=row_ptr, col_idx=col_idx, values=values, nspc=np.ones(nb, np.int32),
+                  rhs=rng.standard_normal(N))

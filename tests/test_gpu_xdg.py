@@ -121,3 +121,15 @@ def test_batch_of_independent_xdg_problems(cuda):
         tol = SOL_TOL if specs[i]["mu"][1] <= 10 else 1e-8     # conditioning bound of the larger jumps
         for name in out:
             assert np.linalg.norm(sols[(name, i)] - xd) <= tol * np.linalg.norm(xd)
+
+
+def test_schwarz_block_covering_everything_is_exact(cuda):
+    """As addSchwarzTest.Test_Solution_IsCorrect (addSchwarzTest.cs:186-202): patches that cover the whole system
+    (complete block graph) make one Schwarz application an exact solve."""
+    from helpers import dense_block_system
+    v = dense_block_system(6, 4, seed=5)
+    op = MultigridOperator(BlockMsrMatrix.from_system(v), MultigridOperator.Eye)
+    x = np.zeros(v.N)
+    SchwarzConfig(FixedNoOfIterations=1).CreateInstance(op).Solve(x, v.rhs)
+    xs = np.linalg.solve(v.to_scipy().toarray(), v.rhs)
+    assert np.linalg.norm(x - xs) <= 1e-13 * np.linalg.norm(xs)

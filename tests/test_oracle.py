@@ -202,3 +202,15 @@ def test_recalc_resi_period_keeps_the_solution():
         r = O.solve(O.Bsr.of(s), s.rhs, cfg)
         assert r.converged
         assert np.linalg.norm(r.x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+def test_schwarz_block_covering_everything_is_exact():
+    """addSchwarzTest.Test_Solution_IsCorrect (AdvancedSolverTestsMPI/Solver/addSchwarzTest.cs:186-202): when a
+    Schwarz block covers the whole system, one application solves it (|x - x*| < 1e-14 there).  With a complete
+    block graph every cell's patch is the whole system, so the restricted factors are the rows of A^{-1}."""
+    from helpers import dense_block_system
+    v = dense_block_system(6, 4, seed=5)
+    M = O.schwarz_rows(O.Bsr.of(v))
+    x = O.spmv(O.Bsr.of(v, values=M), 1.0, v.rhs, 0.0, np.zeros(v.N))
+    xs = np.linalg.solve(v.to_scipy().toarray(), v.rhs)
+    assert np.linalg.norm(x - xs) < 1e-14
