@@ -8,7 +8,8 @@ Names, argument meaning and error behaviour follow the reference:
   ``DiagBlockEquilib`` change of basis (``MultigridOperator_ChangeOfBasis.cs:624``).
 * Solver configurations implement ``ISolverFactory.CreateInstance(MultigridOperator)``
   (``ISmootherTemplate.cs:136-152``): ``FGMRESConfig`` (``FlexGMRES.cs:35``), ``PmgConfig`` (``PmgConfig.cs:80``),
-  ``SoftPCGConfig`` (``SoftPCG.cs:37``), ``BlockJacobiConfig`` (``BlockJacobi.cs:35``).  The returned solver
+  ``SoftPCGConfig`` (``SoftPCG.cs:37``), ``SoftGMRESConfig`` (``SoftGMRES.cs:75``), ``BlockJacobiConfig``
+  (``BlockJacobi.cs:35``), ``SchwarzConfig`` (``Schwarz.cs:424``), ``CellILUConfig`` (``CellILU.cs:22``).  The returned solver
   implements ``ISolverSmootherTemplate`` (``ISmootherTemplate.cs:29-83``): ``Solve(X, B)`` with X the initial
   guess in and the solution out, ``ThisLevelIterations``, ``IterationsInNested``, ``Converged``, ``ResetStat``,
   ``Dispose``.  Non-convergence is not an exception; NaN/Inf or breakdown raise ``ArithmeticError``.
