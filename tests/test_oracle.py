@@ -214,3 +214,16 @@ def test_schwarz_block_covering_everything_is_exact():
     x = O.spmv(O.Bsr.of(v, values=M), 1.0, v.rhs, 0.0, np.zeros(v.N))
     xs = np.linalg.solve(v.to_scipy().toarray(), v.rhs)
     assert np.linalg.norm(x - xs) < 1e-14
+
+
+def test_log_coeff_features():
+    """Learned-stage features: log k of the cell and its six face neighbours (the cell's own value at walls)."""
+    s = A.variable_coeff_3d(4, 1, seed=1)
+    f = A.log_coeff_features(s)
+    assert f.shape == (s.nb, 7) and f.dtype == np.float32
+    lk = np.log(s.coeff)
+    nbr = s.grid.face_neighbours()
+    for c in (0, 21, s.nb - 1):
+        assert np.isclose(f[c, 0], lk[c])
+        for q in range(6):
+            assert np.isclose(f[c, 1 + q], lk[nbr[c, q]] if nbr[c, q] >= 0 else lk[c])

@@ -33,3 +33,23 @@ def test_block_layout_is_consistent():
     for i in range(s.nb):  # sorted, unique block columns with the diagonal present
         c = s.col_idx[s.row_ptr[i]:s.row_ptr[i + 1]]
         assert np.all(np.diff(c) > 0) and i in c
+
+
+def test_batch_specs_are_seeded_and_in_range():
+    a, b = xdg.batch_specs(64, seed=3), xdg.batch_specs(64, seed=3)
+    assert a == b and len(a) == 64
+    for sp in a:
+        assert sp["n"] in xdg.BATCH_EDGES and 0.15 <= sp["radius"] <= 0.35
+        assert sp["mu"][0] == 1.0 and sp["mu"][1] in xdg.BATCH_JUMPS
+        assert all(0.4 <= c <= 0.6 for c in sp["centre"])
+    assert len({sp["n"] for sp in a}) > 1 and len({sp["mu"][1] for sp in a}) > 1
+
+
+def test_xdg_matrix_text_exchange(tmp_path):
+    """An XDG system (blocks of 10 and 20 rows) survives the SaveToTextFileSparse round trip bit for bit."""
+    from bosss_b200 import matrixio
+    s = xdg.xdg_sphere(n=4, p=2, seed=1)
+    path = str(tmp_path / "xdg.txt")
+    matrixio.save_text_sparse(path, s.Np, s.row_ptr, s.col_idx, s.values, s.nspc)
+    M = matrixio.load_text_sparse(path)
+    assert abs(M - s.to_scipy()).max() == 0.0
