@@ -59,3 +59,28 @@ def test_solver_config_defaults_follow_reference():
     assert c.tol == 1e-10 and c.max_iter == 300 and c.min_iter == 1
     assert c.post_sweeps == 10 and c.bj_iters == 1 and c.bj_omega == 1.0
     assert c.sub_max_iter == 100 and c.sub_reduction == 0.1
+
+
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and offsetof of `struct` as the C compiler lays it out from include/bsgpu.h."""
+    src = tmp_path / "layout.c"
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "bsgpu.h"', 'int main(void) {',
+             f'  printf("%zu\\n", sizeof({struct}));']
+    lines += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    lines += ['  return 0;', '}']
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    vals = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    return vals[0], vals[1:]
+
+
+@pytest.mark.parametrize("struct,cls", [("bsgpu_solver_config", nat.SolverConfig),
+                                        ("bsgpu_solve_stats", nat.SolveStats)])
+def test_struct_layouts_match_the_header(tmp_path, struct, cls):
+    """The ctypes mirrors (and so the C# binding text built the same way) lay the structs out as the C compiler."""
+    import ctypes as C
+    names = [f[0] for f in cls._fields_]
+    size, offsets = _c_layout(tmp_path, struct, names)
+    assert size == C.sizeof(cls)
+    assert offsets == [getattr(cls, n).offset for n in names]
