@@ -574,6 +574,98 @@ struct OrthoMG : Solver {
 // `reference_defect` reproduces FlexGMRES.cs:259-260, where the least-squares result is overwritten by
 // alpha = (beta, 0, ..., 0), i.e. X += beta*Z_0; it also checks termination only once per restart, as the
 // reference does (:168-183).  Without it the implicit residual is checked after every Arnoldi step.
+// SoftGMRES.Solve (SoftGMRES.cs:227-460): restarted GMRES(m), left preconditioned (r = M^{-1}(b - A x), Arnoldi
+// on M^{-1} A with modified Gram-Schmidt), Givens rotations (rotmat, :196-210), x += V y at convergence and at
+// each restart; the termination test compares |s_i| (preconditioned residual estimate) with the initial
+// unpreconditioned residual |b - A x0| (:260-268, :372).  At the iteration limit the cycle's update is applied.
+struct SoftGMRES : Solver {
+  const Mat* A;
+  Solver* precond = nullptr;  // owned; nullptr = identity
+  int m = 80;
+  Term term;
+  std::vector<double>* hist = nullptr;
+  SoftGMRES(const Mat* A_, Solver* pc, int m_, Term t) : A(A_), precond(pc), m(m_), term(t) {}
+  ~SoftGMRES() { delete precond; }
+  void apply_pc(const Vec& in, Vec& out) {
+    if (!precond) { out = in; return; }
+    std::fill(out.begin(), out.end(), 0.0);
+    precond->solve(out, in);
+  }
+  static void rotmat(double& c, double& s, double a, double b) {
+    if (b == 0.0) { c = 1.0; s = 0.0; }
+    else if (std::fabs(b) > std::fabs(a)) { double t = a / b; s = 1.0 / std::sqrt(1.0 + t * t); c = t * s; }
+    else { double t = b / a; c = 1.0 / std::sqrt(1.0 + t * t); s = t * c; }
+  }
+  void solve(Vec& X, const Vec& B) override {
+    const size_t L = B.size();
+    Vec z(L), r(L), w(L);
+    z = B;
+    spmv(*A, -1.0, X.data(), 1.0, z.data());
+    const double r0 = nrm2(z);
+    if (hist) hist->push_back(r0);
+    auto t0 = term(0, r0, r0);
+    if (!t0.first) { converged = t0.second; return; }
+    std::vector<Vec> V(m + 1, Vec(L));
+    std::vector<double> H((size_t)(m + 1) * m), cs(m), sn(m), s(m + 2), y(m);
+    int tot = 0;
+    bool first = true;
+    while (true) {
+      if (!first) { z = B; spmv(*A, -1.0, X.data(), 1.0, z.data()); }
+      first = false;
+      apply_pc(z, r);
+      const double beta = nrm2(r);
+      if (!std::isfinite(beta)) throw std::runtime_error("SoftGMRES: NaN/Inf");
+      if (beta == 0.0) { converged = true; break; }
+      V[0] = r;
+      scal(1.0 / beta, V[0]);
+      std::fill(s.begin(), s.end(), 0.0);
+      s[0] = beta;
+      int i;
+      bool stop = false;
+      double err = beta;
+      for (i = 1; i <= m; ++i) {
+        spmv(*A, 1.0, V[i - 1].data(), 0.0, z.data());
+        apply_pc(z, w);
+        for (int k = 0; k < i; ++k) {
+          H[k * m + (i - 1)] = dot(w, V[k]);
+          axpy(-H[k * m + (i - 1)], V[k], w);
+        }
+        const double nw = nrm2(w);
+        H[i * m + (i - 1)] = nw;
+        V[i] = w;
+        if (nw > 0) scal(1.0 / nw, V[i]);
+        for (int k = 1; k <= i - 1; ++k) {
+          const double tmp = cs[k - 1] * H[(k - 1) * m + i - 1] + sn[k - 1] * H[k * m + i - 1];
+          H[k * m + i - 1] = -sn[k - 1] * H[(k - 1) * m + i - 1] + cs[k - 1] * H[k * m + i - 1];
+          H[(k - 1) * m + i - 1] = tmp;
+        }
+        rotmat(cs[i - 1], sn[i - 1], H[(i - 1) * m + i - 1], H[i * m + i - 1]);
+        const double tmp = cs[i - 1] * s[i - 1];
+        H[(i - 1) * m + i - 1] = cs[i - 1] * H[(i - 1) * m + i - 1] + sn[i - 1] * H[i * m + i - 1];
+        H[i * m + i - 1] = 0.0;
+        s[i] = -sn[i - 1] * s[i - 1];
+        s[i - 1] = tmp;
+        err = std::fabs(s[i]);
+        if (hist) hist->push_back(err);
+        auto t1 = term(tot, r0, err);
+        ++tot;
+        if (!t1.first || nw == 0.0) { stop = true; converged = t1.second || nw == 0.0; break; }
+      }
+      const int kk = stop ? i : m;
+      for (int a = kk - 1; a >= 0; --a) {
+        double acc = s[a];
+        for (int q = a + 1; q < kk; ++q) acc -= H[a * m + q] * y[q];
+        y[a] = acc / H[a * m + a];
+      }
+      for (int a = 0; a < kk; ++a) axpy(y[a], V[a], X);
+      if (stop) break;
+      auto t2 = term(tot, r0, err);
+      if (!t2.first) { converged = t2.second; break; }
+    }
+    this_level_iterations = tot;
+  }
+};
+
 struct FlexGMRES : Solver {
   const Mat* A;
   Solver* precond = nullptr;  // owned
@@ -1092,6 +1184,11 @@ int or_solve(const or_bsr* m, const or_solver_cfg* c, const double* b, double* x
       f->reference_defect = c->reference_fgmres_defect != 0;
       f->hist = &h;
       s = f;
+    } else if (c->solver == OR_SOLVER_SOFTGMRES) {
+      auto* g = new SoftGMRES(&A, c->bj_iters >= 0 ? new BlockJacobi(&A, c->bj_iters, c->bj_omega) : nullptr,
+                              c->max_krylov, top);
+      g->hist = &h;
+      s = g;
     } else {
       g_err = "unknown solver kind";
       return OR_ERR_ARGUMENT;

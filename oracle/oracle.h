@@ -4,7 +4,7 @@
 #include <stdint.h>
 
 enum { OR_OK = 0, OR_ERR_ARGUMENT = 1, OR_ERR_ARITHMETIC = 3 };
-enum { OR_SOLVER_PCG = 0, OR_SOLVER_FGMRES_PMG = 1, OR_SOLVER_ORTHOMG = 2 };
+enum { OR_SOLVER_PCG = 0, OR_SOLVER_FGMRES_PMG = 1, OR_SOLVER_ORTHOMG = 2, OR_SOLVER_SOFTGMRES = 3 };
 enum { OR_COARSE_DENSE = 0, OR_COARSE_PCG = 1 };
 
 /* Block-sparse matrix: block i has nspc[i]*Np rows (nspc NULL: 1 species); blocks row-major, concatenated in

@@ -16,7 +16,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
-PCG, FGMRES_PMG, ORTHOMG = 0, 1, 2
+PCG, FGMRES_PMG, ORTHOMG, SOFTGMRES = 0, 1, 2, 3
 COARSE_DENSE, COARSE_PCG = 0, 1
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 

@@ -227,3 +227,24 @@ def test_log_coeff_features():
         assert np.isclose(f[c, 0], lk[c])
         for q in range(6):
             assert np.isclose(f[c, 1 + q], lk[nbr[c, q]] if nbr[c, q] >= 0 else lk[c])
+
+
+@pytest.mark.parametrize("bj", [-1, 0])
+def test_softgmres_restatement(bj):
+    """SoftGMRES (SoftGMRES.cs:227-460) restated: left-preconditioned GMRES(m), without a preconditioner and with
+    block Jacobi, reaches the direct solution.  As in the solver path, it runs on the DiagBlockEquilib operator
+    L A L^T (its termination test compares the preconditioned residual estimate with the unpreconditioned
+    initial residual, which is only meaningful when M^{-1} is of unit scale)."""
+    from helpers import apply_blocks
+    s = A.poisson_3d(4, 2, seed=3)
+    vals, Lc = O.change_of_basis(O.Bsr.of(s))
+
+    class T:
+        Np, row_ptr, col_idx, values = s.Np, s.row_ptr, s.col_idx, vals
+    bl = np.full(s.nb, s.Np)
+    r = O.solve(O.Bsr.of(T), apply_blocks(Lc, bl, s.rhs),
+                O.SolverConfig(solver=O.SOFTGMRES, tol=1e-13, max_krylov=40, max_iter=5000, bj_iters=bj))
+    x = apply_blocks(Lc, bl, r.x, transpose=True)
+    xd = O.direct_solve(s)
+    assert r.converged
+    assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
