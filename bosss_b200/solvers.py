@@ -344,7 +344,9 @@ class SoftGMRESConfig(IterativeSolverConfig):
     block Jacobi / Schwarz), or None.  Left preconditioning needs the same M^{-1} in every application, so the
     p-multigrid V-cycle (which varies between calls) belongs in ``FGMRESConfig``; a ``PmgConfig`` is rejected.
     The termination test compares the preconditioned residual estimate with the unpreconditioned initial
-    residual, as the reference does.
+    residual, as the reference does; that comparison is meaningful when the preconditioner is of unit scale, as
+    block Jacobi is on the DiagBlockEquilib operator (the ``MultigridOperator`` default).  On an unscaled operator
+    with large diagonal blocks the preconditioned estimate falls below the absolute machine-precision floor early.
     """
     MaxKrylovDim: int = 80
     Precond: object = None
