@@ -817,6 +817,203 @@ void load_mat(Mat& A, const or_bsr* m) {
   A.val = m->values;  // external storage, not copied
 }
 
+// Schwarz patch inverses restated for patches = one cell plus the cells of its block row (Schwarz.cs:623-840):
+// the rows of the centre cell of each patch inverse, in A's layout.
+int schwarz_rows_mat(const Mat& A, double* values_out) {
+  {
+    int err = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : err)
+    for (int64_t K = 0; K < A.nb; ++K) {
+      std::vector<int32_t> cells(A.ci.begin() + A.rp[K], A.ci.begin() + A.rp[K + 1]);
+      std::vector<int> off(cells.size() + 1, 0);
+      for (size_t a = 0; a < cells.size(); ++a) off[a + 1] = off[a] + A.len[cells[a]];
+      const int n = off.back();
+      std::vector<double> P((size_t)n * n, 0.0);
+      for (size_t a = 0; a < cells.size(); ++a) {
+        const int32_t ca = cells[a];
+        for (int64_t q = A.rp[ca]; q < A.rp[ca + 1]; ++q) {
+          auto it = std::find(cells.begin(), cells.end(), A.ci[q]);
+          if (it == cells.end()) continue;
+          const size_t b = it - cells.begin();
+          const int I = A.len[ca], J = A.len[A.ci[q]];
+          const double* blk = A.blk(q);
+          for (int r = 0; r < I; ++r)
+            for (int c = 0; c < J; ++c) P[(size_t)(off[a] + r) * n + off[b] + c] = blk[r * J + c];
+        }
+      }
+      err |= invert(n, P.data());
+      const size_t aK = std::find(cells.begin(), cells.end(), (int32_t)K) - cells.begin();
+      const int I = A.len[K];
+      for (size_t b = 0; b < cells.size(); ++b) {
+        const int J = A.len[cells[b]];
+        double* o = values_out + A.vp[A.rp[K] + b];
+        for (int r = 0; r < I; ++r)
+          for (int c = 0; c < J; ++c) o[r * J + c] = P[(size_t)(off[aK] + r) * n + off[b] + c];
+      }
+    }
+    if (err) { g_err = "Schwarz: singular block"; return OR_ERR_ARITHMETIC; }
+    return 0;
+  }
+}
+
+
+// helpers of the block ILU(0) restatement
+void gemm_sub(int I, int K, int J, const double* A, const double* B, double* C) {  // C -= A B, row-major
+  for (int r = 0; r < I; ++r)
+    for (int k = 0; k < K; ++k) {
+      const double a = A[r * K + k];
+      for (int c = 0; c < J; ++c) C[r * J + c] -= a * B[k * J + c];
+    }
+}
+int64_t find_block(const Mat& A, int64_t i, int32_t j) {
+  const int32_t* b = A.ci.data() + A.rp[i];
+  const int32_t* e = A.ci.data() + A.rp[i + 1];
+  const int32_t* p = std::lower_bound(b, e, j);
+  return (p != e && *p == j) ? A.rp[i] + (p - b) : -1;
+}
+std::vector<int64_t> positions(const Mat& A, const int32_t* order) {
+  std::vector<int64_t> pos(A.nb);
+  for (int64_t q = 0; q < A.nb; ++q) pos[order ? order[q] : q] = q;
+  return pos;
+}
+
+int ilu0_factor_mat(const Mat& A, const int32_t* order, double* factor_out) {
+  {
+    std::vector<int64_t> pos = positions(A, order);
+    std::copy(A.val, A.val + A.vp[A.nnzb()], factor_out);
+    auto W = [&](int64_t k) { return factor_out + A.vp[k]; };
+    for (int64_t kk = 0; kk + 1 < A.nb; ++kk) {
+      const int64_t k = order ? order[kk] : kk;
+      const int Sk = A.len[k];
+      if (Sk == 0) continue;
+      const int64_t dkk = find_block(A, k, (int32_t)k);
+      if (dkk < 0) continue;
+      std::vector<double> inv(W(dkk), W(dkk) + (size_t)Sk * Sk);
+      if (invert(Sk, inv.data()) != 0) continue;
+      // rows i > k (in the ordering) with an occupied block (i, k); the pattern is structurally symmetric
+      for (int64_t q = A.rp[k]; q < A.rp[k + 1]; ++q) {
+        const int64_t i = A.ci[q];
+        if (pos[i] <= pos[k]) continue;
+        const int64_t qik = find_block(A, i, (int32_t)k);
+        if (qik < 0) continue;
+        const int Si = A.len[i];
+        std::vector<double> L((size_t)Si * Sk, 0.0);
+        gemm_sub(Si, Sk, Sk, W(qik), inv.data(), L.data());          // L = -A_ik inv(A_kk)
+        for (auto& v : L) v = -v;
+        std::copy(L.begin(), L.end(), W(qik));
+        for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+          const int32_t j = A.ci[p];
+          if (pos[j] <= pos[k]) continue;
+          const int64_t qkj = find_block(A, k, j);
+          if (qkj < 0) continue;                                      // (k, j) outside the ILU(0) pattern
+          gemm_sub(Si, Sk, A.len[j], L.data(), W(qkj), W(p));
+        }
+      }
+    }
+    return 0;
+  }
+}
+
+
+int ilu0_solve_mat(const Mat& A, const int32_t* order, const double* factor, const double* b, double* x) {
+  {
+    std::vector<int64_t> pos = positions(A, order);
+    std::vector<double> y(b, b + A.N);
+    for (int64_t q = 0; q < A.nb; ++q) {
+      const int64_t i = order ? order[q] : q;
+      const int I = A.len[i];
+      for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+        const int32_t k = A.ci[p];
+        if (pos[k] >= pos[i]) continue;
+        const int K = A.len[k];
+        const double* L = factor + A.vp[p];
+        for (int r = 0; r < I; ++r)
+          for (int c = 0; c < K; ++c) y[A.i0[i] + r] -= L[r * K + c] * y[A.i0[k] + c];
+      }
+    }
+    for (int64_t q = A.nb - 1; q >= 0; --q) {
+      const int64_t i = order ? order[q] : q;
+      const int I = A.len[i];
+      std::vector<double> s(y.begin() + A.i0[i], y.begin() + A.i0[i] + I);
+      for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
+        const int32_t j = A.ci[p];
+        if (pos[j] <= pos[i]) continue;
+        const int J = A.len[j];
+        const double* U = factor + A.vp[p];
+        for (int r = 0; r < I; ++r)
+          for (int c = 0; c < J; ++c) s[r] -= U[r * J + c] * x[A.i0[j] + c];
+      }
+      const int64_t d = find_block(A, i, (int32_t)i);
+      if (d < 0) { g_err = "ILU: missing diagonal block"; return OR_ERR_ARGUMENT; }
+      std::vector<double> inv(factor + A.vp[d], factor + A.vp[d] + (size_t)I * I);
+      if (invert(I, inv.data()) != 0) { g_err = "ILU: singular diagonal block"; return OR_ERR_ARITHMETIC; }
+      for (int r = 0; r < I; ++r) {
+        double acc = 0.0;
+        for (int c = 0; c < I; ++c) acc += inv[r * I + c] * s[c];
+        x[A.i0[i] + r] = acc;
+      }
+    }
+    return 0;
+  }
+}
+
+
+// Restricted additive Schwarz smoother (Schwarz.cs:996-1147 with the patches of schwarz_rows_mat):
+// x <- x + M (b - A x), FixedNoOfIterations = iters + 1 updates.
+struct SchwarzSmoother : Solver {
+  const Mat* A;
+  Mat M;
+  int updates;
+  SchwarzSmoother(const Mat* A_, int iters) : A(A_), M(*A_), updates(iters + 1) {
+    M.v.assign(A->vp.back(), 0.0);
+    M.val = M.v.data();
+    if (schwarz_rows_mat(*A, M.v.data()) != 0) throw std::runtime_error("Schwarz: singular block");
+  }
+  void solve(Vec& x, const Vec& b) override {
+    Vec r(b.size());
+    for (int s = 0; s < updates; ++s) {
+      r = b;
+      spmv(*A, -1.0, x.data(), 1.0, r.data());
+      spmv(M, 1.0, r.data(), 1.0, x.data());
+    }
+    converged = true;
+  }
+};
+
+// Block ILU(0) smoother (CellILU.Solve, CellILU.cs:182-250): x = U^{-1} L^{-1} b with the factors computed in the
+// natural cell order (the reference's) or with the cells ordered by a greedy colouring of the block graph (colour
+// 0 first; the order the GPU smoother uses).
+struct ILUSmoother : Solver {
+  const Mat* A;
+  std::vector<double> F;
+  std::vector<int32_t> order;
+  ILUSmoother(const Mat* A_, bool coloured) : A(A_) {
+    if (coloured) {
+      std::vector<int32_t> col(A->nb, -1);
+      int ncol = 0;
+      for (int64_t i = 0; i < A->nb; ++i) {
+        std::vector<char> used(ncol + 1, 0);
+        for (int64_t k = A->rp[i]; k < A->rp[i + 1]; ++k)
+          if (A->ci[k] != i && col[A->ci[k]] >= 0) used[col[A->ci[k]]] = 1;
+        int cc = 0;
+        while (cc < ncol && used[cc]) ++cc;
+        col[i] = cc;
+        if (cc == ncol) ++ncol;
+      }
+      for (int cc = 0; cc < ncol; ++cc)
+        for (int64_t i = 0; i < A->nb; ++i)
+          if (col[i] == cc) order.push_back((int32_t)i);
+    }
+    F.assign(A->vp.back(), 0.0);
+    ilu0_factor_mat(*A, order.empty() ? nullptr : order.data(), F.data());
+  }
+  void solve(Vec& x, const Vec& b) override {
+    if (ilu0_solve_mat(*A, order.empty() ? nullptr : order.data(), F.data(), b.data(), x.data()) != 0)
+      throw std::runtime_error("ILU: singular pivot block");
+    converged = true;
+  }
+};
+
 Solver* build_level(const Mat* A, const or_solver_cfg* c, int level, std::vector<Restriction*>& keep);
 
 Solver* make_coarsest(const Mat* A, const or_solver_cfg* c) {
@@ -847,7 +1044,12 @@ Solver* build_level(const Mat* A, const or_solver_cfg* c, int level, std::vector
   auto* omg = new OrthoMG(A, t);
   omg->ortho.recalc_period = c->recalc_resi_period;
   omg->sweeps = c->post_sweeps;
-  omg->post = new BlockJacobi(A, c->bj_iters, c->bj_omega);
+  if (c->smoother == OR_SMOOTHER_SCHWARZ)
+    omg->post = new SchwarzSmoother(A, c->bj_iters);
+  else if (c->smoother == OR_SMOOTHER_ILU_COLOURED || c->smoother == OR_SMOOTHER_ILU_NATURAL)
+    omg->post = new ILUSmoother(A, c->smoother == OR_SMOOTHER_ILU_COLOURED);
+  else
+    omg->post = new BlockJacobi(A, c->bj_iters, c->bj_omega);
   auto* gr = new GridAndDegRestriction(A, c->level_keep[level + 1]);
   gr->lower = build_level(&gr->R.sub, c, level + 1, keep);
   omg->coarse = gr;
@@ -922,38 +1124,7 @@ int or_schwarz_rows(const or_bsr* m, double* values_out) {
   try {
     Mat A;
     load_mat(A, m);
-    int err = 0;
-#pragma omp parallel for schedule(dynamic, 64) reduction(| : err)
-    for (int64_t K = 0; K < A.nb; ++K) {
-      std::vector<int32_t> cells(A.ci.begin() + A.rp[K], A.ci.begin() + A.rp[K + 1]);
-      std::vector<int> off(cells.size() + 1, 0);
-      for (size_t a = 0; a < cells.size(); ++a) off[a + 1] = off[a] + A.len[cells[a]];
-      const int n = off.back();
-      std::vector<double> P((size_t)n * n, 0.0);
-      for (size_t a = 0; a < cells.size(); ++a) {
-        const int32_t ca = cells[a];
-        for (int64_t q = A.rp[ca]; q < A.rp[ca + 1]; ++q) {
-          auto it = std::find(cells.begin(), cells.end(), A.ci[q]);
-          if (it == cells.end()) continue;
-          const size_t b = it - cells.begin();
-          const int I = A.len[ca], J = A.len[A.ci[q]];
-          const double* blk = A.blk(q);
-          for (int r = 0; r < I; ++r)
-            for (int c = 0; c < J; ++c) P[(size_t)(off[a] + r) * n + off[b] + c] = blk[r * J + c];
-        }
-      }
-      err |= invert(n, P.data());
-      const size_t aK = std::find(cells.begin(), cells.end(), (int32_t)K) - cells.begin();
-      const int I = A.len[K];
-      for (size_t b = 0; b < cells.size(); ++b) {
-        const int J = A.len[cells[b]];
-        double* o = values_out + A.vp[A.rp[K] + b];
-        for (int r = 0; r < I; ++r)
-          for (int c = 0; c < J; ++c) o[r * J + c] = P[(size_t)(off[aK] + r) * n + off[b] + c];
-      }
-    }
-    if (err) { g_err = "Schwarz: singular block"; return OR_ERR_ARITHMETIC; }
-    return 0;
+    return schwarz_rows_mat(A, values_out);
   } catch (std::exception& e) {
     g_err = e.what();
     return OR_ERR_ARGUMENT;
@@ -964,63 +1135,11 @@ int or_schwarz_rows(const or_bsr* m, double* values_out) {
 // in-place KIJ form over the block rows taken in the order `order` (NULL: natural order, the reference's).
 // factor_out receives the factors in A's layout: strictly lower blocks L_ik (unit lower factor), upper blocks and
 // the diagonal U_ij.  A diagonal block whose factorisation fails is skipped, as the reference does.
-namespace {
-void gemm_sub(int I, int K, int J, const double* A, const double* B, double* C) {  // C -= A B, row-major
-  for (int r = 0; r < I; ++r)
-    for (int k = 0; k < K; ++k) {
-      const double a = A[r * K + k];
-      for (int c = 0; c < J; ++c) C[r * J + c] -= a * B[k * J + c];
-    }
-}
-int64_t find_block(const Mat& A, int64_t i, int32_t j) {
-  const int32_t* b = A.ci.data() + A.rp[i];
-  const int32_t* e = A.ci.data() + A.rp[i + 1];
-  const int32_t* p = std::lower_bound(b, e, j);
-  return (p != e && *p == j) ? A.rp[i] + (p - b) : -1;
-}
-std::vector<int64_t> positions(const Mat& A, const int32_t* order) {
-  std::vector<int64_t> pos(A.nb);
-  for (int64_t q = 0; q < A.nb; ++q) pos[order ? order[q] : q] = q;
-  return pos;
-}
-}  // namespace
-
 int or_ilu0_factor(const or_bsr* m, const int32_t* order, double* factor_out) {
   try {
     Mat A;
     load_mat(A, m);
-    std::vector<int64_t> pos = positions(A, order);
-    std::copy(A.val, A.val + A.vp[A.nnzb()], factor_out);
-    auto W = [&](int64_t k) { return factor_out + A.vp[k]; };
-    for (int64_t kk = 0; kk + 1 < A.nb; ++kk) {
-      const int64_t k = order ? order[kk] : kk;
-      const int Sk = A.len[k];
-      if (Sk == 0) continue;
-      const int64_t dkk = find_block(A, k, (int32_t)k);
-      if (dkk < 0) continue;
-      std::vector<double> inv(W(dkk), W(dkk) + (size_t)Sk * Sk);
-      if (invert(Sk, inv.data()) != 0) continue;
-      // rows i > k (in the ordering) with an occupied block (i, k); the pattern is structurally symmetric
-      for (int64_t q = A.rp[k]; q < A.rp[k + 1]; ++q) {
-        const int64_t i = A.ci[q];
-        if (pos[i] <= pos[k]) continue;
-        const int64_t qik = find_block(A, i, (int32_t)k);
-        if (qik < 0) continue;
-        const int Si = A.len[i];
-        std::vector<double> L((size_t)Si * Sk, 0.0);
-        gemm_sub(Si, Sk, Sk, W(qik), inv.data(), L.data());          // L = -A_ik inv(A_kk)
-        for (auto& v : L) v = -v;
-        std::copy(L.begin(), L.end(), W(qik));
-        for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
-          const int32_t j = A.ci[p];
-          if (pos[j] <= pos[k]) continue;
-          const int64_t qkj = find_block(A, k, j);
-          if (qkj < 0) continue;                                      // (k, j) outside the ILU(0) pattern
-          gemm_sub(Si, Sk, A.len[j], L.data(), W(qkj), W(p));
-        }
-      }
-    }
-    return 0;
+    return ilu0_factor_mat(A, order, factor_out);
   } catch (std::exception& e) {
     g_err = e.what();
     return OR_ERR_ARGUMENT;
@@ -1033,43 +1152,7 @@ int or_ilu0_solve(const or_bsr* m, const int32_t* order, const double* factor, c
   try {
     Mat A;
     load_mat(A, m);
-    std::vector<int64_t> pos = positions(A, order);
-    std::vector<double> y(b, b + A.N);
-    for (int64_t q = 0; q < A.nb; ++q) {
-      const int64_t i = order ? order[q] : q;
-      const int I = A.len[i];
-      for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
-        const int32_t k = A.ci[p];
-        if (pos[k] >= pos[i]) continue;
-        const int K = A.len[k];
-        const double* L = factor + A.vp[p];
-        for (int r = 0; r < I; ++r)
-          for (int c = 0; c < K; ++c) y[A.i0[i] + r] -= L[r * K + c] * y[A.i0[k] + c];
-      }
-    }
-    for (int64_t q = A.nb - 1; q >= 0; --q) {
-      const int64_t i = order ? order[q] : q;
-      const int I = A.len[i];
-      std::vector<double> s(y.begin() + A.i0[i], y.begin() + A.i0[i] + I);
-      for (int64_t p = A.rp[i]; p < A.rp[i + 1]; ++p) {
-        const int32_t j = A.ci[p];
-        if (pos[j] <= pos[i]) continue;
-        const int J = A.len[j];
-        const double* U = factor + A.vp[p];
-        for (int r = 0; r < I; ++r)
-          for (int c = 0; c < J; ++c) s[r] -= U[r * J + c] * x[A.i0[j] + c];
-      }
-      const int64_t d = find_block(A, i, (int32_t)i);
-      if (d < 0) { g_err = "ILU: missing diagonal block"; return OR_ERR_ARGUMENT; }
-      std::vector<double> inv(factor + A.vp[d], factor + A.vp[d] + (size_t)I * I);
-      if (invert(I, inv.data()) != 0) { g_err = "ILU: singular diagonal block"; return OR_ERR_ARITHMETIC; }
-      for (int r = 0; r < I; ++r) {
-        double acc = 0.0;
-        for (int c = 0; c < I; ++c) acc += inv[r * I + c] * s[c];
-        x[A.i0[i] + r] = acc;
-      }
-    }
-    return 0;
+    return ilu0_solve_mat(A, order, factor, b, x);
   } catch (std::exception& e) {
     g_err = e.what();
     return OR_ERR_ARGUMENT;

@@ -6,6 +6,7 @@
 enum { OR_OK = 0, OR_ERR_ARGUMENT = 1, OR_ERR_ARITHMETIC = 3 };
 enum { OR_SOLVER_PCG = 0, OR_SOLVER_FGMRES_PMG = 1, OR_SOLVER_ORTHOMG = 2, OR_SOLVER_SOFTGMRES = 3 };
 enum { OR_COARSE_DENSE = 0, OR_COARSE_PCG = 1 };
+enum { OR_SMOOTHER_BLOCKJACOBI = 0, OR_SMOOTHER_SCHWARZ = 1, OR_SMOOTHER_ILU_COLOURED = 2, OR_SMOOTHER_ILU_NATURAL = 3 };
 
 /* Block-sparse matrix: block i has nspc[i]*Np rows (nspc NULL: 1 species); blocks row-major, concatenated in
  * BSR order (block rows ascending, block columns ascending). */
@@ -35,6 +36,7 @@ typedef struct {
   double sub_reduction;
   int32_t reference_fgmres_defect;
   int32_t recalc_resi_period; /* OrthoMG RecalcResiPeriod (OrthonormalizationMultigrid.cs:211); <= 1: every update */
+  int32_t smoother;           /* OR_SMOOTHER_*: post-smoother of the p-levels */
 } or_solver_cfg;
 
 typedef struct {

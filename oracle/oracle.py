@@ -18,6 +18,7 @@ _LIB = None
 
 PCG, FGMRES_PMG, ORTHOMG, SOFTGMRES = 0, 1, 2, 3
 COARSE_DENSE, COARSE_PCG = 0, 1
+SMOOTHER_BLOCKJACOBI, SMOOTHER_SCHWARZ, SMOOTHER_ILU_COLOURED, SMOOTHER_ILU_NATURAL = 0, 1, 2, 3
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 
 
@@ -32,7 +33,7 @@ class _Cfg(C.Structure):
                 ("level_keep", C.c_int32 * 8), ("post_sweeps", C.c_int32), ("bj_iters", C.c_int32),
                 ("bj_omega", C.c_double), ("coarse_kind", C.c_int32), ("coarse_tol", C.c_double),
                 ("coarse_max_iter", C.c_int32), ("sub_max_iter", C.c_int32), ("sub_reduction", C.c_double),
-                ("reference_fgmres_defect", C.c_int32), ("recalc_resi_period", C.c_int32)]
+                ("reference_fgmres_defect", C.c_int32), ("recalc_resi_period", C.c_int32), ("smoother", C.c_int32)]
 
 
 class _Stats(C.Structure):
@@ -207,6 +208,7 @@ class SolverConfig:
     sub_reduction: float = 0.1
     reference_fgmres_defect: bool = False
     recalc_resi_period: int = 1
+    smoother: int = SMOOTHER_BLOCKJACOBI
 
     def _c(self) -> _Cfg:
         c = _Cfg()
@@ -220,6 +222,7 @@ class SolverConfig:
         c.sub_max_iter, c.sub_reduction = self.sub_max_iter, self.sub_reduction
         c.reference_fgmres_defect = int(bool(self.reference_fgmres_defect))
         c.recalc_resi_period = int(self.recalc_resi_period)
+        c.smoother = int(self.smoother)
         return c
 
 

@@ -248,3 +248,23 @@ def test_softgmres_restatement(bj):
     xd = O.direct_solve(s)
     assert r.converged
     assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("smoother", [O.SMOOTHER_SCHWARZ, O.SMOOTHER_ILU_COLOURED, O.SMOOTHER_ILU_NATURAL])
+def test_pmg_with_schwarz_and_ilu_smoothers(smoother):
+    """p-multigrid post-smoothing with restricted Schwarz and with block ILU(0) (natural and two-colour order):
+    FlexGMRES reaches the direct solution on the equilibrated operator."""
+    from helpers import apply_blocks
+    s = A.poisson_3d(4, 2, seed=6)
+    vals, Lc = O.change_of_basis(O.Bsr.of(s))
+
+    class T:
+        Np, row_ptr, col_idx, values = s.Np, s.row_ptr, s.col_idx, vals
+    bl = np.full(s.nb, s.Np)
+    cfg = O.SolverConfig(solver=O.FGMRES_PMG, tol=1e-12, level_keep=(10, 4), post_sweeps=4, coarse_tol=1e-2,
+                         smoother=smoother)
+    r = O.solve(O.Bsr.of(T), apply_blocks(Lc, bl, s.rhs), cfg)
+    x = apply_blocks(Lc, bl, r.x, transpose=True)
+    xd = O.direct_solve(s)
+    assert r.converged
+    assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
