@@ -112,15 +112,15 @@ class BatchSolver:
                 times = {}
                 errors = []
 
-                def work(i, w):
+                def work(i, w, key):
                     try:
                         a = time.perf_counter()
-                        w["slv"][name].Solve(w["X"][name], w["B"])
+                        w["slv"][key].Solve(w["X"][key], w["B"])
                         times[i] = time.perf_counter() - a
                     except Exception as e:  # re-raised on the calling thread
                         errors.append(e)
 
-                threads = [threading.Thread(target=work, args=(i, w)) for i, w in wave]
+                threads = [threading.Thread(target=work, args=(i, w, name)) for i, w in wave]
                 a = time.perf_counter()
                 for t in threads:
                     t.start()
