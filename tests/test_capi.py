@@ -84,3 +84,22 @@ def test_struct_layouts_match_the_header(tmp_path, struct, cls):
     size, offsets = _c_layout(tmp_path, struct, names)
     assert size == C.sizeof(cls)
     assert offsets == [getattr(cls, n).offset for n in names]
+
+
+def test_argument_errors_need_no_device():
+    """Null handles and bad sizes are BSGPU_ERR_ARGUMENT (the reference's ArgumentException), reported before any
+    device work; destroying a null handle is a no-op."""
+    import ctypes as C
+    L = nat.lib()
+    h = C.c_void_p()
+    assert L.bsgpu_matrix_create(C.byref(h), 4, 2, None, None, None, None, 0) == nat.ERR_ARGUMENT
+    assert L.bsgpu_matrix_create(C.byref(h), -1, 2, None, None, None, None, 0) == nat.ERR_ARGUMENT
+    assert "nb" in nat.last_error()
+    assert L.bsgpu_solver_config_default(None) == nat.ERR_ARGUMENT
+    assert L.bsgpu_solver_create(C.byref(h), None, None) == nat.ERR_ARGUMENT
+    assert L.bsgpu_solver_solve(None, None, None, None) == nat.ERR_ARGUMENT
+    assert L.bsgpu_matrix_spmv(None, 1.0, None, 0.0, None) == nat.ERR_ARGUMENT
+    assert L.bsgpu_matrix_spmv_noalloc(None, 1.0, None, 0.0, None) == nat.ERR_ARGUMENT
+    assert L.bsgpu_matrix_destroy(None) == 0 and L.bsgpu_solver_destroy(None) == 0 and L.bsgpu_mgop_destroy(None) == 0
+    with pytest.raises(ValueError):
+        nat.check(nat.ERR_ARGUMENT)
