@@ -268,3 +268,17 @@ def test_pmg_with_schwarz_and_ilu_smoothers(smoother):
     xd = O.direct_solve(s)
     assert r.converged
     assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("D,p", [(2, 2), (3, 1)])
+def test_h_prolongation_is_polynomial_exact(D, p):
+    """Agglomeration prolongation (the h-levels of the coarse solver): a degree-p polynomial's coarse projection,
+    prolongated, is its fine projection (the MG transfer exactness of TestProgramLinearMG.cs:166,308-309)."""
+    g = A.uniform_grid(D, 4)
+    P = A.h_prolongation(g, p)
+    f = lambda X: 1.0 + 0.5 * X[0] - 0.3 * X[-1] + (0.7 * X[0] * X[-1] if p >= 2 else 0.0)
+    cf = A.project_function(g, p, f, q=p + 3)
+    cc = A.project_function(P.coarse_grid, p, f, q=p + 3)
+    vals = np.asarray(P.values).reshape(P.nb_fine, P.Np, P.Np)
+    got = np.stack([vals[i] @ cc[P.col_idx[i]] for i in range(P.nb_fine)])
+    assert np.abs(got - cf).max() <= 1e-12 * np.abs(cf).max()
