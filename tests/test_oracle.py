@@ -282,3 +282,13 @@ def test_h_prolongation_is_polynomial_exact(D, p):
     vals = np.asarray(P.values).reshape(P.nb_fine, P.Np, P.Np)
     got = np.stack([vals[i] @ cc[P.col_idx[i]] for i in range(P.nb_fine)])
     assert np.abs(got - cf).max() <= 1e-12 * np.abs(cf).max()
+
+
+def test_sip_operators_are_symmetric_and_coefficient_scaled():
+    """The SIP operators are symmetric; a constant diffusivity k scales the operator by k (ipLaplace.cs:95-245)."""
+    s = A.poisson_3d(3, 2)
+    M = s.to_scipy()
+    assert abs(M - M.T).max() <= 1e-12 * abs(M).max()
+    g = A.uniform_grid(3, 3)
+    k = A.assemble_sip(g, 2, penalty=12.0, coeff=np.full(g.ncells, 2.5)).to_scipy()
+    assert abs(k - 2.5 * M).max() <= 1e-12 * abs(M).max()
