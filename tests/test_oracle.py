@@ -292,3 +292,26 @@ def test_sip_operators_are_symmetric_and_coefficient_scaled():
     g = A.uniform_grid(3, 3)
     k = A.assemble_sip(g, 2, penalty=12.0, coeff=np.full(g.ncells, 2.5)).to_scipy()
     assert abs(k - 2.5 * M).max() <= 1e-12 * abs(M).max()
+
+
+def test_natural_order_ilu_parallelises_by_wavefronts():
+    """Block ILU(0) in the reference's natural order depends only on lower neighbours, so the rows of one wavefront
+    (level = 1 + max level of the lower neighbours) can be factored together: any order inside a wavefront gives the
+    same factors up to the order in which a diagonal block receives its updates (rounding only), and an n^3
+    Cartesian grid has 3n - 2 wavefronts."""
+    s = A.poisson_3d(4, 1, seed=7)
+    nb = s.nb
+    level = np.zeros(nb, np.int64)
+    for i in range(nb):
+        lower = [j for j in s.col_idx[s.row_ptr[i]:s.row_ptr[i + 1]] if j < i]
+        level[i] = 1 + max((level[j] for j in lower), default=-1)
+    assert level.max() + 1 == 3 * 4 - 2
+    Bo = O.Bsr.of(s)
+    F_nat = O.ilu0_factor(Bo)
+    # wavefront order with each wavefront reversed: a different sequential order with the same dependencies
+    order = np.concatenate([np.nonzero(level == L)[0][::-1] for L in range(level.max() + 1)]).astype(np.int32)
+    F_wave = O.ilu0_factor(Bo, order)
+    assert np.abs(F_nat - F_wave).max() <= 1e-14 * np.abs(F_nat).max()
+    b = np.random.default_rng(0).standard_normal(s.N)
+    x1, x2 = O.ilu0_solve(Bo, F_nat, b), O.ilu0_solve(Bo, F_wave, b, order)
+    assert np.abs(x1 - x2).max() <= 1e-12 * np.abs(x1).max()
