@@ -53,3 +53,21 @@ def test_xdg_matrix_text_exchange(tmp_path):
     matrixio.save_text_sparse(path, s.Np, s.row_ptr, s.col_idx, s.values, s.nspc)
     M = matrixio.load_text_sparse(path)
     assert abs(M - s.to_scipy()).max() == 0.0
+
+
+def test_workload_fingerprints():
+    """The seeded workload generators reproduce the committed fingerprints (tests/golden/make_workload_fingerprints.py)."""
+    import json
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    from make_workload_fingerprints import fingerprints
+    ref = json.load(open(os.path.join(here, "workload_fingerprints.json")))
+    got = fingerprints()
+    assert set(got) == set(ref)
+    for name, r in ref.items():
+        g = got[name]
+        assert g["N"] == r["N"] and g["nnzb"] == r["nnzb"], name
+        for k in ("values_l2", "values_sum", "rhs_l2", "rhs_sum"):
+            assert abs(g[k] - r[k]) <= 1e-10 * max(1.0, abs(r[k])), (name, k)
