@@ -30,6 +30,7 @@ struct bsgpu_solver_s {
   bsgpu::DBuf<double> X, B, Xt, Bt;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   std::vector<double> history;
+  double* lscal = nullptr;  // device scalars of the learned-stage entry points
 };
 
 namespace bsgpu {
@@ -345,6 +346,8 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->learned_stall = 0.99;
     cfg->ortho_max_krylov = 96;
     cfg->recalc_resi_period = 1;
+    cfg->learned_pairs = 0;
+    cfg->graph = 0;
   });
 }
 
@@ -443,6 +446,76 @@ BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len) {
     out += "]";
     std::strncpy(buf, out.c_str(), len - 1);
     buf[len - 1] = '\0';
+  });
+}
+
+static LearnedNet& learned_of(bsgpu_solver_t s) {
+  require(s != nullptr, "null solver");
+  require(s->tree->net != nullptr, "the solver was created without the learned stage (cfg.learned = 0)");
+  return *s->tree->net;
+}
+
+BSGPU_API int bsgpu_solver_learned_info(bsgpu_solver_t s, int32_t* dims) {
+  return guarded([&] {
+    LearnedNet& n = learned_of(s);
+    require(dims != nullptr, "null argument");
+    const int32_t d[8] = {n.Np, n.nfaces, n.nextra, n.F, n.Fp, n.H, n.Op, s->tree->learned_pool};
+    std::memcpy(dims, d, sizeof(d));
+  });
+}
+
+BSGPU_API int bsgpu_solver_learned_get_weights(bsgpu_solver_t s, float* w1, float* w2, float* w3) {
+  return guarded([&] {
+    LearnedNet& n = learned_of(s);
+    require(w1 && w2 && w3, "null argument");
+    BSGPU_CUDA(cudaStreamSynchronize(s->tree->ctx->st));
+    learned_get_weights(n, w1, w2, w3);
+  });
+}
+
+BSGPU_API int bsgpu_solver_learned_set_weights(bsgpu_solver_t s, const float* w1, const float* w2, const float* w3) {
+  return guarded([&] {
+    LearnedNet& n = learned_of(s);
+    require(w1 && w2 && w3, "null argument");
+    BSGPU_CUDA(cudaStreamSynchronize(s->tree->ctx->st));
+    learned_set_weights(n, w1, w2, w3);
+  });
+}
+
+BSGPU_API int bsgpu_solver_learned_apply(bsgpu_solver_t s, const double* r, double* z) {
+  return guarded([&] {
+    LearnedNet& n = learned_of(s);
+    require(r && z, "null argument");
+    Ctx& c = *s->tree->ctx;
+    const int64_t N = n.ncells * n.Np;
+    BSGPU_CUDA(cudaMemcpyAsync(s->B.p, r, N * 8, cudaMemcpyHostToDevice, c.st));
+    if (!s->lscal) s->lscal = c.scal(8);
+    double* d = s->lscal;
+    const double* a[1] = {s->B.p};
+    dots(c.red, 1, a, a, N, d, 1, c.st);
+    learned_scale(d, d + 1, N, c.st);
+    learned_apply(n, s->B.p, s->X.p, d + 1, c.st);
+    BSGPU_CUDA(cudaMemcpyAsync(z, s->X.p, N * 8, cudaMemcpyDeviceToHost, c.st));
+    BSGPU_CUDA(cudaStreamSynchronize(c.st));
+  });
+}
+
+BSGPU_API int bsgpu_solver_learned_gradient(bsgpu_solver_t s, const double* r, float* g1, float* g2, float* g3,
+                                            double* loss) {
+  return guarded([&] {
+    LearnedNet& n = learned_of(s);
+    require(r && g1 && g2 && g3, "null argument");
+    Ctx& c = *s->tree->ctx;
+    const int64_t N = n.ncells * n.Np;
+    DBuf<double> Az(std::max<int64_t>(N, 1)), g(std::max<int64_t>(N, 1));
+    BSGPU_CUDA(cudaMemcpyAsync(s->B.p, r, N * 8, cudaMemcpyHostToDevice, c.st));
+    if (!s->lscal) s->lscal = c.scal(8);
+    double* scal = s->lscal;
+    learned_gradient(n, *s->tree->A, s->B.p, s->X.p, Az.p, g.p, c.red, scal, c.st);
+    learned_take_gradient(n, g1, g2, g3, c.st);
+    c.fetch(scal, 5);
+    const double* h = c.hscal + (scal - c.dscal.p);
+    if (loss) *loss = (h[3] - 2.0 * h[4]) / h[2];
   });
 }
 

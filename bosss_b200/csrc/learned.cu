@@ -350,8 +350,50 @@ void learned_apply(const LearnedNet& net, const float* r, float* z, const double
   apply_impl<float>(net, r, z, scale, nullptr, st);
 }
 
-void learned_train_step(LearnedNet& net, const Matrix& A, const double* r, double* z, double* Az, double* g,
-                        ReduceScratch& red, double* scal, double lr, cudaStream_t st) {
+void learned_get_weights(const LearnedNet& net, float* w1, float* w2, float* w3) {
+  auto get = [](const DBuf<uint16_t>& b, float* out) {
+    std::vector<uint16_t> h(b.n);
+    BSGPU_CUDA(cudaMemcpy(h.data(), b.p, b.n * 2, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < h.size(); ++i) {
+      const uint32_t u = (uint32_t)h[i] << 16;
+      std::memcpy(out + i, &u, 4);
+    }
+  };
+  get(net.w1, w1);
+  get(net.w2, w2);
+  get(net.w3, w3);
+}
+
+void learned_set_weights(LearnedNet& net, const float* w1, const float* w2, const float* w3) {
+  auto set = [](const float* in, DBuf<float>& master, DBuf<uint16_t>& b, DBuf<float>& grad, DBuf<float>& m,
+                DBuf<float>& v) {
+    std::vector<uint16_t> hb(master.n);
+    for (size_t i = 0; i < hb.size(); ++i) hb[i] = to_bf16_bits(in[i]);
+    BSGPU_CUDA(cudaMemcpy(master.p, in, master.n * 4, cudaMemcpyHostToDevice));
+    BSGPU_CUDA(cudaMemcpy(b.p, hb.data(), hb.size() * 2, cudaMemcpyHostToDevice));
+    BSGPU_CUDA(cudaMemset(grad.p, 0, grad.n * 4));
+    BSGPU_CUDA(cudaMemset(m.p, 0, m.n * 4));
+    BSGPU_CUDA(cudaMemset(v.p, 0, v.n * 4));
+  };
+  set(w1, net.m1, net.w1, net.g1, net.a1, net.v1);
+  set(w2, net.m2, net.w2, net.g2, net.a2, net.v2);
+  set(w3, net.m3, net.w3, net.g3, net.a3, net.v3);
+  net.adam_t = 0;
+}
+
+void learned_take_gradient(LearnedNet& net, float* g1, float* g2, float* g3, cudaStream_t st) {
+  auto take = [&](DBuf<float>& g, float* out) {
+    BSGPU_CUDA(cudaMemcpyAsync(out, g.p, g.n * 4, cudaMemcpyDeviceToHost, st));
+    BSGPU_CUDA(cudaMemsetAsync(g.p, 0, g.n * 4, st));
+  };
+  take(net.g1, g1);
+  take(net.g2, g2);
+  take(net.g3, g3);
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+}
+
+void learned_gradient(LearnedNet& net, const Matrix& A, const double* r, double* z, double* Az, double* g,
+                      ReduceScratch& red, double* scal, cudaStream_t st) {
   // scal: [0] |r|, [1] scale, [2] |r|^2, [3] z.Az, [4] z.r
   const int64_t N = net.ncells * net.Np;
   if (!net.act.p) net.act.alloc((size_t)net.ncells * 2 * net.H);
@@ -376,6 +418,11 @@ void learned_train_step(LearnedNet& net, const Matrix& A, const double* r, doubl
   const int bgrid = (int)std::min<int64_t>((net.ncells + kBTile - 1) / kBTile, (int64_t)num_sms());
   mlp_bwd_kernel<<<bgrid, 256, sm, st>>>(b, r);
   BSGPU_CHECK_LAUNCH();
+}
+
+void learned_train_step(LearnedNet& net, const Matrix& A, const double* r, double* z, double* Az, double* g,
+                        ReduceScratch& red, double* scal, double lr, cudaStream_t st) {
+  learned_gradient(net, A, r, z, Az, g, red, scal, st);
   net.adam_t++;
   const float b1 = 0.9f, b2 = 0.999f;
   const float c1 = 1.0f - std::pow(b1, (float)net.adam_t), c2 = 1.0f - std::pow(b2, (float)net.adam_t);

@@ -39,5 +39,16 @@ void learned_scale(const double* nrm, double* scale, int64_t n, cudaStream_t st)
 // Returns the loss through a device scalar (loss_out).
 void learned_train_step(LearnedNet& net, const Matrix& A, const double* r, double* z, double* Az, double* g,
                         ReduceScratch& red, double* scal, double lr, cudaStream_t st);
+// The same loss and its gradient without the update: the gradient is accumulated into net.g1..g3 (which must be
+// zero), the loss terms into scal[0..4] as above.
+void learned_gradient(LearnedNet& net, const Matrix& A, const double* r, double* z, double* Az, double* g,
+                      ReduceScratch& red, double* scal, cudaStream_t st);
+// Host copies of the weights the kernels use (BF16, widened exactly to float; padded shapes Fp x H, H x H, H x Op,
+// row-major), and replacement of the weights (FP32 master copies = the given values, BF16 copies rounded to
+// nearest even; Adam state reset).
+void learned_get_weights(const LearnedNet& net, float* w1, float* w2, float* w3);
+void learned_set_weights(LearnedNet& net, const float* w1, const float* w2, const float* w3);
+// Copies the accumulated gradient to the host and zeroes it.
+void learned_take_gradient(LearnedNet& net, float* g1, float* g2, float* g3, cudaStream_t st);
 
 }  // namespace bsgpu

@@ -1681,17 +1681,18 @@ double train_learned(Tree& t, int n_rhs, int steps, double lr, uint64_t seed) {
   const bool was_on = t.learned_on;
   t.learned_on = false;
   t.collect = &pool;
-  t.collect_cap = (size_t)n_rhs * 12;
+  // cfg.learned_pairs residuals in total (default 12 per right-hand side), spread evenly over the solves
+  const size_t pairs = t.cfg.learned_pairs > 0 ? (size_t)t.cfg.learned_pairs : (size_t)n_rhs * 12;
+  const size_t per = (pairs + n_rhs - 1) / n_rhs;
   DBuf<double> b(std::max<int64_t>(N, 1)), x(std::max<int64_t>(N, 1));
-  for (int k = 0; k < n_rhs; ++k) {
+  for (int k = 0; k < n_rhs && pool.size() < pairs; ++k) {
     fill_random(b.p, N, seed + 7919ull * k, c.st);
     fill(0.0, x.p, N, c.st);
-    const size_t before = pool.size();
-    t.collect_cap = before + 12;
+    t.collect_cap = std::min(pairs, pool.size() + per);
     t.top->solve(c, x.p, b.p, true);
-    (void)before;
   }
   t.collect = nullptr;
+  t.learned_pool = (int)pool.size();
   require(!pool.empty(), "no training residuals were generated");
   // 2. Adam on the energy-norm loss
   DBuf<double> z(N), Az(N), g(N);

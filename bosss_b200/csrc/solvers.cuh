@@ -111,6 +111,7 @@ struct Tree {
   std::vector<DBuf<double>>* collect = nullptr;
   size_t collect_cap = 0;
   int learned_stalls = 0;           // solves in which the learned stage stalled and was switched off
+  int learned_pool = 0;             // training residuals collected by the last train_learned
 };
 Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info);
 // Generates training residuals with the solver itself (FGMRES Arnoldi vectors of solves with seeded random

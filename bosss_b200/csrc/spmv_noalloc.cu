@@ -4,10 +4,14 @@
 // callers cannot have that: a host program that has handed the GPU's memory to its own pool (or runs under a
 // hard device-memory budget) must not see the library grow its footprint, and cudaMalloc/cudaFree may
 // synchronise the whole device, which a caller on a latency-critical path cannot afford.  This variant stages x
-// and y in one file-scope __device__ array instead.  That array is part of the module image: every GPU that loads
-// the library holds it (2 x 8 MiB) until the process exits, whether or not this entry point is ever called.
+// and y in one file-scope __device__ array instead.  That array is part of the module image: once the library's
+// module is loaded on a GPU (at its first use there under CUDA's default lazy loading), that GPU holds the array
+// (2 x 8 MiB) until the process exits, whether or not this entry point is ever called.  The device address is
+// cached per device ordinal, so resetting a device's primary context (cudaDeviceReset) invalidates this entry
+// point on that device for the rest of the process, as it invalidates every matrix handle.
 #include <map>
 #include <mutex>
+#include <new>
 
 #include "matrix.cuh"
 
@@ -68,6 +72,9 @@ extern "C" BSGPU_API int bsgpu_matrix_spmv_noalloc(bsgpu_matrix_t A, double alph
   } catch (const bsgpu::Error& e) {
     bsgpu::set_last_error(e.what());
     return e.code;
+  } catch (const std::bad_alloc&) {
+    bsgpu::set_last_error("host allocation failed");
+    return BSGPU_ERR_NOMEM;
   } catch (const std::exception& e) {
     bsgpu::set_last_error(e.what());
     return BSGPU_ERR_ARGUMENT;

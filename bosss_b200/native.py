@@ -32,6 +32,8 @@ EXPORTS = [
     "bsgpu_solver_train_learned",
     "bsgpu_solver_config_default", "bsgpu_solver_create", "bsgpu_solver_destroy", "bsgpu_solver_solve",
     "bsgpu_solver_solve_device", "bsgpu_solver_get_history", "bsgpu_solver_set_tracing", "bsgpu_solver_get_trace",
+    "bsgpu_solver_learned_info", "bsgpu_solver_learned_get_weights", "bsgpu_solver_learned_set_weights",
+    "bsgpu_solver_learned_apply", "bsgpu_solver_learned_gradient",
 ]
 
 
@@ -44,7 +46,8 @@ class SolverConfig(C.Structure):
                 ("precision", C.c_int32), ("h_levels", C.c_int32), ("h_sweeps", C.c_int32), ("h_cycle", C.c_int32),
                 ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
                 ("learned", C.c_int32), ("learned_hidden", C.c_int32), ("learned_stall", C.c_double),
-                ("ortho_max_krylov", C.c_int32), ("recalc_resi_period", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("ortho_max_krylov", C.c_int32), ("recalc_resi_period", C.c_int32), ("learned_pairs", C.c_int32),
+                ("graph", C.c_int32), ("reserved", C.c_int32 * 2)]
 
 
 class SolveStats(C.Structure):
@@ -107,6 +110,11 @@ def lib() -> C.CDLL:
             "bsgpu_solver_get_history": [vp, vp, i32, vp],
             "bsgpu_solver_set_tracing": [vp, i32],
             "bsgpu_solver_get_trace": [vp, C.c_char_p, C.c_size_t],
+            "bsgpu_solver_learned_info": [vp, vp],
+            "bsgpu_solver_learned_get_weights": [vp, vp, vp, vp],
+            "bsgpu_solver_learned_set_weights": [vp, vp, vp, vp],
+            "bsgpu_solver_learned_apply": [vp, vp, vp],
+            "bsgpu_solver_learned_gradient": [vp, vp, vp, vp, vp, vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

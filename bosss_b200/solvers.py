@@ -317,6 +317,7 @@ class FGMRESConfig(IterativeSolverConfig):
     Learned: str = "off"            # "off" | "fgmres" | "presmooth" | "both"; needs MultigridOperator.SetCellGraph
     LearnedHidden: int = 64
     LearnedStall: float = 0.99
+    LearnedPairs: int = 0           # training residuals collected in total (0: 12 per right-hand side)
 
     def _config(self):
         if len(self.Preconditioners) != 1:
@@ -333,6 +334,9 @@ class FGMRESConfig(IterativeSolverConfig):
         c.learned = modes[self.Learned]
         c.learned_hidden = self.LearnedHidden
         c.learned_stall = self.LearnedStall
+        if self.LearnedPairs < 0:
+            raise ValueError("LearnedPairs must be >= 0")
+        c.learned_pairs = self.LearnedPairs
         return c
 
 
@@ -500,6 +504,44 @@ class GpuSolver:
         nat.check(nat.lib().bsgpu_solver_train_learned(self._h, int(n_rhs), int(steps), float(lr), int(seed),
                                                        C.byref(loss)))
         return loss.value
+
+    def LearnedInfo(self) -> dict:
+        d = (C.c_int32 * 8)()
+        nat.check(nat.lib().bsgpu_solver_learned_info(self._h, d))
+        return dict(zip(("Np", "nfaces", "nextra", "F", "Fp", "H", "Op", "pairs"), list(d)))
+
+    def LearnedWeights(self):
+        """(W1 [Fp x H], W2 [H x H], W3 [H x Op]): the BF16 weights of the learned stage as float32."""
+        i = self.LearnedInfo()
+        w = [np.zeros((i["Fp"], i["H"]), np.float32), np.zeros((i["H"], i["H"]), np.float32),
+             np.zeros((i["H"], i["Op"]), np.float32)]
+        nat.check(nat.lib().bsgpu_solver_learned_get_weights(self._h, *(nat.ptr(a) for a in w)))
+        return w
+
+    def SetLearnedWeights(self, w1, w2, w3):
+        w = [np.ascontiguousarray(a, np.float32) for a in (w1, w2, w3)]
+        i = self.LearnedInfo()
+        if [a.shape for a in w] != [(i["Fp"], i["H"]), (i["H"], i["H"]), (i["H"], i["Op"])]:
+            raise ValueError("learned-stage weight shapes do not match")
+        nat.check(nat.lib().bsgpu_solver_learned_set_weights(self._h, *(nat.ptr(a) for a in w)))
+
+    def ApplyLearned(self, r) -> np.ndarray:
+        """One application of the learned stage to r (operator basis, host vector)."""
+        r = np.ascontiguousarray(r, np.float64)
+        z = np.zeros_like(r)
+        nat.check(nat.lib().bsgpu_solver_learned_apply(self._h, nat.ptr(r), nat.ptr(z)))
+        return z
+
+    def LearnedGradient(self, r):
+        """(loss, [dL/dW1, dL/dW2, dL/dW3]) of the training loss for one residual r; no update."""
+        i = self.LearnedInfo()
+        r = np.ascontiguousarray(r, np.float64)
+        g = [np.zeros((i["Fp"], i["H"]), np.float32), np.zeros((i["H"], i["H"]), np.float32),
+             np.zeros((i["H"], i["Op"]), np.float32)]
+        loss = C.c_double()
+        nat.check(nat.lib().bsgpu_solver_learned_gradient(self._h, nat.ptr(r), *(nat.ptr(a) for a in g),
+                                                          C.byref(loss)))
+        return loss.value, g
 
     def SetTracing(self, on: bool = True):
         nat.check(nat.lib().bsgpu_solver_set_tracing(self._h, 1 if on else 0))

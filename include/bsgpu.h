@@ -80,9 +80,11 @@ BSGPU_API int bsgpu_matrix_spmv(bsgpu_matrix_t A, double alpha, const double* x,
 /* Same as bsgpu_matrix_spmv but allocates no device memory, for callers that must not (a host program whose
  * device memory is already committed to its own pool, or one that cannot afford the device-wide synchronisation
  * cudaMalloc/cudaFree may cause).  No counterpart in the reference.  x and y are staged in a fixed array of
- * 2 x 2^20 doubles that every GPU loading the library holds until exit, so nrows must be <= 1,048,576
- * (BSGPU_ERR_ARGUMENT otherwise).  The first call on a device looks up that array's device address, so make it
- * before any stream capture.  All calls share the array: calls that overlap on the GPU (several host threads)
+ * 2 x 2^20 doubles (16 MiB) that a GPU holds from the moment the library's module is loaded on it (its first use
+ * there, under CUDA's lazy loading) until exit, whether or not this function is called; nrows must be
+ * <= 1,048,576 (BSGPU_ERR_ARGUMENT otherwise).  The first call on a device looks up that array's device address,
+ * so make it before any stream capture; a reset of the device's primary context invalidates the cached address
+ * (as it does every handle).  All calls share the array: calls that overlap on the GPU (several host threads)
  * race. */
 BSGPU_API int bsgpu_matrix_spmv_noalloc(bsgpu_matrix_t A, double alpha, const double* x, double beta, double* y);
 /* Same on device vectors, asynchronous on `stream` (NULL = the legacy default stream). */
@@ -181,7 +183,10 @@ typedef struct {
                                the current iterate (default 96)                                  */
   int32_t recalc_resi_period; /* OrthoMG RecalcResiPeriod (OrthonormalizationMultigrid.cs:211): the residual is
                                  recomputed from scratch every this many history entries, else updated (default 1) */
-  int32_t reserved[4];
+  int32_t learned_pairs;    /* training residuals bsgpu_solver_train_learned collects in total, spread over its
+                               n_rhs solves (0: 12 per right-hand side)                           */
+  int32_t graph;            /* reserved (0)                                                     */
+  int32_t reserved[2];
 } bsgpu_solver_config;
 
 typedef struct {
@@ -215,6 +220,22 @@ BSGPU_API int bsgpu_solver_set_tracing(bsgpu_solver_t s, int32_t on);
 BSGPU_API int bsgpu_solver_train_learned(bsgpu_solver_t s, int32_t n_rhs, int32_t steps, double lr, uint64_t seed,
                                          double* loss);
 BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len);
+
+/* ---- learned stage access (no counterpart in the reference) --------------------------------------------- *
+ * For checking and exchanging the trained network.  dims[8]: Np, nfaces, nextra, F (input width), Fp (F padded
+ * to 16), H (hidden width), Op (Np padded to 16), residuals collected by the last training.  Weights are the
+ * padded row-major matrices W1 [Fp x H], W2 [H x H], W3 [H x Op] of z_c = W3^T relu(W2^T relu(W1^T f_c)), f_c =
+ * [r_c, r of the face neighbours in table order (0 where none), cell features, 0 padding]; get returns the BF16
+ * values the kernels use, set stores FP32 masters and their BF16 roundings.  apply evaluates the stage once on a
+ * host vector r in the operator's (transformed) basis: z = s NN(r / s), s = |r| / sqrt(n).  gradient evaluates the
+ * training loss (z^T A z - 2 z^T r) / |r|^2 for one r and its gradient with respect to W1, W2, W3 (host buffers of
+ * the padded shapes) without updating the weights. */
+BSGPU_API int bsgpu_solver_learned_info(bsgpu_solver_t s, int32_t* dims);
+BSGPU_API int bsgpu_solver_learned_get_weights(bsgpu_solver_t s, float* w1, float* w2, float* w3);
+BSGPU_API int bsgpu_solver_learned_set_weights(bsgpu_solver_t s, const float* w1, const float* w2, const float* w3);
+BSGPU_API int bsgpu_solver_learned_apply(bsgpu_solver_t s, const double* r, double* z);
+BSGPU_API int bsgpu_solver_learned_gradient(bsgpu_solver_t s, const double* r, float* g1, float* g2, float* g3,
+                                            double* loss);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,147 @@
+"""Solution fixtures of the configured workloads, computed by the oracle (the CPU restatement, FP64).
+
+For every case the oracle solves the DiagBlockEquilib-transformed system (the operator the solvers see) with
+FlexGMRES(30) + p-multigrid to a relative residual far below the solvers' 1e-10, the solution is mapped back to the
+original basis (X = L^T X~), and the file keeps what a GPU test needs to compare a solution of the full system
+without shipping it: the L2 norm, a seeded sample of 10,000 entries (indices and values), the iteration count and
+the residual reached.  The right-hand side is scaled before the solve so that the relative tolerance stays above
+the absolute floor 2.2e-13 of DefaultTermination (IterativeSolverConfig.cs:48-62); the solution is scaled back.
+
+The default case also records the outer iteration count and time of the oracle at the benchmark's own settings
+(tolerance 1e-10 and every SOLVER_PARAMS entry of bench.py, RecalcResiPeriod included) in c2_oracle_solve.json:
+the reference arm of bench.py multiplies its per-iteration sample by that count.
+
+    python tests/golden/make_solution_fixtures.py c2 [c1 c3 c4s c4]
+
+Cases: c1 = 2-D 64^2 p=2 (direct solve), c2 = 3-D 64^3 p=3, c3 = XDG sphere 48^3 p=2 (jump 1:1000),
+c4s = variable coefficient 32^3 p=2, c4 = variable coefficient 96^3 p=2.  c2 takes ~30 min, c4 ~1 h on 8 cores.
+"""
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+
+SAMPLE = 10_000
+SAMPLE_SEED = 20261203
+
+
+def block_len(s):
+    nspc = getattr(s, "nspc", None)
+    nb = len(s.row_ptr) - 1
+    return (np.ones(nb, np.int64) if nspc is None else np.asarray(nspc, np.int64)) * int(s.Np)
+
+
+def apply_blocks(L, v, lens, transpose):
+    """Per-block product with the concatenated row-major I x I blocks L (L v or L^T v)."""
+    out = np.empty_like(v)
+    if np.all(lens == lens[0]):
+        n = int(lens[0])
+        Lb = L.reshape(-1, n, n)
+        sub = "cji,cj->ci" if transpose else "cij,cj->ci"
+        return np.einsum(sub, Lb, v.reshape(-1, n)).reshape(-1)
+    off_v = np.concatenate([[0], np.cumsum(lens)])
+    off_l = np.concatenate([[0], np.cumsum(lens * lens)])
+    for n in np.unique(lens):
+        idx = np.nonzero(lens == n)[0]
+        Lb = np.stack([L[off_l[i]:off_l[i + 1]].reshape(n, n) for i in idx])
+        vb = np.stack([v[off_v[i]:off_v[i + 1]] for i in idx])
+        r = np.einsum("cji,cj->ci" if transpose else "cij,cj->ci", Lb, vb)
+        for k, i in enumerate(idx):
+            out[off_v[i]:off_v[i + 1]] = r[k]
+    return out
+
+
+def system(case):
+    from bosss_b200 import assembly as A
+    from bosss_b200 import xdg
+    if case == "c1":
+        return A.poisson_2d_c1(seed=0), None
+    if case == "c2":
+        return A.poisson_3d(64, 3, seed=0), (20, 10, 4)
+    if case == "c3":
+        return xdg.xdg_sphere(n=48, p=2, seed=0), (10, 4, 1)
+    if case == "c4s":
+        return A.variable_coeff_3d(32, 2, seed=0), (10, 4, 1)
+    if case == "c4":
+        return A.variable_coeff_3d(96, 2, seed=0), (10, 4, 1)
+    raise ValueError(case)
+
+
+def oracle_krylov(s, levels, tol, scale_to=1e4, **kw):
+    """FGMRES + p-MG on the transformed system; returns (X in the original basis, result, seconds)."""
+    Bs = O.Bsr.of(s)
+    vals, L = O.change_of_basis(Bs)
+
+    class T:
+        Np, row_ptr, col_idx, values = s.Np, s.row_ptr, s.col_idx, vals
+        nspc = getattr(s, "nspc", None)
+    lens = block_len(s)
+    bt = apply_blocks(L, np.asarray(s.rhs, np.float64), lens, transpose=False)
+    scale = scale_to / np.linalg.norm(bt) if scale_to else 1.0
+    cfg = O.SolverConfig(solver=O.FGMRES_PMG, tol=tol, top_mode=O.TERM_RELATIVE, level_keep=levels,
+                         coarse_kind=O.COARSE_PCG, max_iter=600, **kw)
+    ps = O.PersistentSolver(O.Bsr.of(T), cfg)
+    t0 = time.perf_counter()
+    r = ps.solve(bt * scale)
+    dt = time.perf_counter() - t0
+    x = apply_blocks(L, r.x / scale, lens, transpose=True)
+    return x, r, dt
+
+
+def sample_of(x):
+    rng = np.random.default_rng(SAMPLE_SEED)
+    idx = np.sort(rng.choice(len(x), size=min(SAMPLE, len(x)), replace=False)).astype(np.int64)
+    return idx, x[idx].copy()
+
+
+def write_solution(case, x, info):
+    idx, vals = sample_of(x)
+    np.savez_compressed(os.path.join(HERE, f"{case}_solution.npz"), idx=idx, values=vals,
+                        norm=np.float64(np.linalg.norm(x)), N=np.int64(len(x)),
+                        info=np.array(json.dumps(info)))
+    print(case, info, flush=True)
+
+
+def main(cases):
+    threads = O.set_threads(os.cpu_count() or 1)
+    from bench import SOLVER_PARAMS, TOL
+    bench_kw = dict(coarse_tol=SOLVER_PARAMS["CoarseTolerance"], coarse_max_iter=SOLVER_PARAMS["CoarseMaxIterations"],
+                    sub_reduction=SOLVER_PARAMS["SubLevelReduction"], sub_max_iter=SOLVER_PARAMS["SubLevelMaxIterations"],
+                    recalc_resi_period=SOLVER_PARAMS["RecalcResiPeriod"], post_sweeps=SOLVER_PARAMS["NoOfPostSmootherSweeps"],
+                    bj_iters=SOLVER_PARAMS["BlockJacobiIterations"])
+    for case in cases:
+        s, levels = system(case)
+        if case == "c1":
+            t0 = time.perf_counter()
+            x = O.direct_solve(s)
+            write_solution(case, x, {"method": "FP64 SuperLU direct solve with 2 refinement steps",
+                                     "seconds": time.perf_counter() - t0, "N": int(s.N)})
+            continue
+        if case == "c2":
+            # the benchmark's own settings, from a zero guess to 1e-10: the reference arm's iteration count
+            _, r, dt = oracle_krylov(s, levels, TOL, scale_to=None, **bench_kw)
+            out = {"iterations": r.iterations, "converged": r.converged, "seconds": dt, "threads": threads,
+                   "relres_transformed": r.res / r.res0, "tol": TOL, "settings": SOLVER_PARAMS,
+                   "workload": "3-D SIP Poisson 64^3 p=3, seed 0"}
+            with open(os.path.join(HERE, "c2_oracle_solve.json"), "w") as f:
+                json.dump(out, f, indent=1)
+            print(out, flush=True)
+        tol = 1e-13
+        x, r, dt = oracle_krylov(s, levels, tol, **bench_kw)
+        write_solution(case, x, {"method": f"oracle FlexGMRES(30) + p-MG {levels}, FP64, block-Jacobi smoothing",
+                                 "tol_relative": tol, "relres_transformed": r.res / r.res0,
+                                 "iterations": r.iterations, "converged": r.converged, "seconds": dt,
+                                 "threads": threads, "N": int(s.N)})
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or ["c2"])

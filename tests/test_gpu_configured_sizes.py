@@ -1,0 +1,149 @@
+"""GPU solutions of the configured workloads at their full sizes, against the oracle.
+
+The fixtures in tests/golden/*_solution.npz hold, for each full-size system, the oracle's FP64 solution (the CPU
+restatement's FlexGMRES + p-multigrid to a relative residual of 1e-13, or an FP64 direct solve for the 2-D case)
+as its L2 norm and a seeded sample of 10,000 entries; tests/golden/make_solution_fixtures.py wrote them.  Each test
+assembles the same seeded system, solves it on the GPU through the C ABI with the benchmark's settings, and
+compares: relative L2 difference on the sample and of the norm.
+
+Tolerances: 1e-9 (the solution criterion of the path) for the Poisson systems.  The XDG sphere with its 1:1000
+diffusivity jump and the variable-coefficient system (k = exp(g), g of variance 1, a contrast of ~1e3 across the
+domain) are much worse conditioned; their solutions at a relative residual of 1e-10 carry the error that the
+conditioning allows, and they are held to the tolerance written beside each case.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from bosss_b200 import assembly as A
+from bosss_b200.solvers import BlockMsrMatrix, FGMRESConfig, MultigridOperator, PmgConfig, SoftPCGConfig
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+SOL_TOL = 1e-9
+# the benchmark's p-multigrid settings (bench.py SOLVER_PARAMS / PMG_SCHWARZ), restated so that the tests do not
+# import the benchmark
+PMG_BJ = dict(NoOfPostSmootherSweeps=10, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.1,
+              CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, RecalcResiPeriod=40)
+PMG_SCHWARZ = dict(PMG_BJ, NoOfPostSmootherSweeps=4, Smoother="schwarz")
+
+
+def fixture(case):
+    path = os.path.join(GOLDEN, f"{case}_solution.npz")
+    if not os.path.exists(path):
+        pytest.fail(f"missing fixture {path} (tests/golden/make_solution_fixtures.py {case})")
+    d = np.load(path)
+    return d["idx"], d["values"], float(d["norm"]), int(d["N"]), json.loads(str(d["info"]))
+
+
+def compare(x, case):
+    idx, vals, norm, N, info = fixture(case)
+    assert len(x) == N
+    sample_err = np.linalg.norm(x[idx] - vals) / np.linalg.norm(vals)
+    norm_err = abs(np.linalg.norm(x) - norm) / norm
+    return sample_err, norm_err
+
+
+def fgmres(op, levels, pmg, mixed, tol=1e-10):
+    return FGMRESConfig(ConvergenceCriterion=tol, termination="relative", MaxKrylovDim=30, MaxSolverIterations=300,
+                        Preconditioners=[PmgConfig(DegreeHierarchy=levels, **pmg)],
+                        MixedPrecision=mixed).CreateInstance(op)
+
+
+def solve(slv, s):
+    import torch
+    B = torch.from_numpy(np.asarray(s.rhs, np.float64)).cuda()
+    X = torch.zeros_like(B)
+    slv.Solve(X, B)
+    return X.cpu().numpy()
+
+
+def test_c1_full_size_softpcg_vs_direct_solve(cuda):
+    """2-D 64^2 p = 2 (24,576 unknowns): block-Jacobi PCG to 1e-10 against the FP64 direct solve, and the
+    iteration count of the oracle's PCG on the same transformed system."""
+    s = A.poisson_2d_c1(seed=0)
+    assert s.N == 24576
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    slv = SoftPCGConfig(ConvergenceCriterion=1e-10, termination="relative",
+                        MaxSolverIterations=20000).CreateInstance(op)
+    x = np.zeros(s.N)
+    slv.Solve(x, s.rhs)
+    assert slv.Converged
+    e_sample, e_norm = compare(x, "c1")
+    assert e_sample <= SOL_TOL and e_norm <= SOL_TOL, (e_sample, e_norm)
+    xd = O.direct_solve(s)
+    assert np.linalg.norm(x - xd) <= SOL_TOL * np.linalg.norm(xd)
+    vals, Lc = O.change_of_basis(O.Bsr.of(s))
+
+    class T:
+        Np, row_ptr, col_idx, values = s.Np, s.row_ptr, s.col_idx, vals
+    from helpers import apply_blocks
+    r = O.solve(O.Bsr.of(T), apply_blocks(Lc, np.full(s.nb, s.Np), s.rhs),
+                O.SolverConfig(solver=O.PCG, tol=1e-10, top_mode=O.TERM_RELATIVE, bj_iters=0, max_iter=20000))
+    assert abs(r.iterations - slv.ThisLevelIterations) <= max(3, 0.02 * r.iterations)
+
+
+@pytest.fixture(scope="module")
+def c2():
+    s = A.poisson_3d(64, 3, seed=0)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    yield s, op
+    op.Dispose()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_c2_full_size_solution_vs_oracle(cuda, c2, mixed):
+    """3-D 64^3 p = 3 (5.24M unknowns), the benchmark's solve (FlexGMRES(30) + p-MG 3 -> 2 -> 1, block-Jacobi,
+    relative residual 1e-10), FP64 and mixed precision, against the oracle's solution; the FP64 path also against
+    the oracle's outer iteration count at the same settings."""
+    s, op = c2
+    slv = fgmres(op, (20, 10, 4), PMG_BJ, mixed)
+    x = solve(slv, s)
+    assert slv.Converged
+    e_sample, e_norm = compare(x, "c2")
+    print(f"c2 mixed={mixed}: iterations {slv.ThisLevelIterations}, sample {e_sample:.3e}, norm {e_norm:.3e}")
+    assert e_sample <= SOL_TOL and e_norm <= SOL_TOL, (e_sample, e_norm)
+    ref = json.load(open(os.path.join(GOLDEN, "c2_oracle_solve.json")))
+    assert ref["settings"]["RecalcResiPeriod"] == PMG_BJ["RecalcResiPeriod"]
+    if not mixed:
+        assert abs(slv.ThisLevelIterations - ref["iterations"]) <= 2, (slv.ThisLevelIterations, ref["iterations"])
+    slv.Dispose()
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_c3_xdg48_solution_vs_oracle(cuda, mixed):
+    """XDG sphere 48^3 p = 2 (two species in cut cells, 1:1000 jump): FP64 block-Jacobi p-MG and FP32 Schwarz
+    p-MG inside FlexGMRES to 1e-10, against the oracle's solution.  Tolerance 1e-7: the condition number of this
+    system (~1e10) turns the residual 1e-10 into solution differences of that order."""
+    from bosss_b200 import xdg
+    s = xdg.xdg_sphere(n=48, p=2, seed=0)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    slv = fgmres(op, (10, 4, 1), PMG_SCHWARZ if mixed else PMG_BJ, mixed)
+    x = solve(slv, s)
+    assert slv.Converged
+    e_sample, e_norm = compare(x, "c3")
+    print(f"c3 mixed={mixed}: iterations {slv.ThisLevelIterations}, sample {e_sample:.3e}, norm {e_norm:.3e}")
+    assert e_sample <= 1e-7 and e_norm <= 1e-7, (e_sample, e_norm)
+    slv.Dispose()
+    op.Dispose()
+
+
+@pytest.mark.parametrize("n,case,mixed", [(32, "c4s", False), (32, "c4s", True), (96, "c4", True)])
+def test_c4_variable_coefficient_solution_vs_oracle(cuda, n, case, mixed):
+    """k = exp(g) diffusion, p = 2, at 32^3 and the configured 96^3 (8.85M unknowns): FP64 block-Jacobi p-MG and
+    FP32 Schwarz p-MG inside FlexGMRES to 1e-10, against the oracle's solution.  Tolerance 1e-8 (coefficient
+    contrast ~1e3 on top of the h^-2 conditioning of the operator)."""
+    s = A.variable_coeff_3d(n, 2, seed=0)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    slv = fgmres(op, (10, 4, 1), PMG_SCHWARZ if mixed else PMG_BJ, mixed)
+    x = solve(slv, s)
+    assert slv.Converged
+    e_sample, e_norm = compare(x, case)
+    print(f"{case} mixed={mixed}: iterations {slv.ThisLevelIterations}, sample {e_sample:.3e}, norm {e_norm:.3e}")
+    assert e_sample <= 1e-8 and e_norm <= 1e-8, (e_sample, e_norm)
+    slv.Dispose()
+    op.Dispose()
