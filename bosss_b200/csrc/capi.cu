@@ -94,6 +94,7 @@ void solve_device(bsgpu_solver_s* s, double* dX, const double* dB, bsgpu_solve_s
   from_transformed(s->op, s->Xt.p, dX, c.st);
   BSGPU_CUDA(cudaEventRecord(s->e1, c.st));
   BSGPU_CUDA(cudaEventSynchronize(s->e1));
+  c.flush_graph_counts();
   float ms = 0;
   BSGPU_CUDA(cudaEventElapsedTime(&ms, s->e0, s->e1));
   s->history = t.top->history;
@@ -137,6 +138,23 @@ BSGPU_API int bsgpu_last_error(char* buf, size_t len) {
 
 BSGPU_API int bsgpu_set_device(int device) {
   return guarded([&] { BSGPU_CUDA(cudaSetDevice(device)); });
+}
+
+BSGPU_API int bsgpu_matrix_autotune(bsgpu_matrix_t A) {
+  return guarded([&] {
+    require(A != nullptr && A->get() != nullptr, "null matrix");
+    autotune(*A->get(), 0, nullptr, nullptr);
+    BSGPU_CUDA(cudaStreamSynchronize(nullptr));
+  });
+}
+
+BSGPU_API int bsgpu_autotune_report(char* buf, size_t len) {
+  return guarded([&] {
+    require(buf != nullptr && len > 0, "null argument");
+    const std::string r = autotune_report();
+    std::strncpy(buf, r.c_str(), len - 1);
+    buf[len - 1] = '\0';
+  });
 }
 
 BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, const int32_t* nspc,
@@ -348,6 +366,7 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->recalc_resi_period = 1;
     cfg->learned_pairs = 0;
     cfg->graph = 0;
+    cfg->autotune = 0;
   });
 }
 

@@ -1,6 +1,9 @@
 // Block-sparse matrix storage and the SpMV family (BlockMsrMatrix.SpMV, BlockMsrMatrix.cs:2970-3410).
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <numeric>
+#include <sstream>
 
 #include "ldst.cuh"
 #include "matrix.cuh"
@@ -90,7 +93,7 @@ __global__ void restrict_kernel(const T* __restrict__ in, const int64_t* __restr
 template <typename T>
 struct Acc { using type = T; };
 
-// Uniform Np x Np blocks, Np known at compile time.  A CTA owns BPC = 256/NP whole block rows; thread t is DOF
+// Uniform Np x Np blocks, Np known at compile time.  A CTA owns BPC = blockDim/NP whole block rows; thread t is DOF
 // row r = t % NP of block row t / NP.  MODE 0: y = alpha*A*x + beta*z.  MODE 1: fused block-Jacobi update
 // y = x + alpha * Dinv * (z - A*x) (z = b), the block row's residual exchanged through shared memory.
 template <typename T, int NP, int V, int MODE>
@@ -98,9 +101,9 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
     const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const T* __restrict__ vals,
     const T* x, const T* __restrict__ z, T* y, T alpha, T beta, int64_t nb,
     const T* __restrict__ dinv, const int* __restrict__ active, const int32_t* __restrict__ row_list = nullptr) {
-  constexpr int BPC = 256 / NP;
   static_assert(NP % V == 0, "chunk width must divide the block size");
   if (active != nullptr && *active == 0) return;
+  const int BPC = blockDim.x / NP;  // block rows per CTA (the launch shape the autotuner picks)
   const int t = threadIdx.x;
   const int lb = t / NP;
   const int r = t - lb * NP;
@@ -227,6 +230,97 @@ __global__ void __launch_bounds__(256) spmv_general_kernel(
   }
 }
 
+// Blocks of one or two species of NP modes each (XDG cut cells carry two).  The block rows of one species count are
+// listed in `rows`; a CTA owns blockDim / (NS*NP) of them, thread t being DOF row r of list entry t / (NS*NP), as in
+// the uniform kernel, so the row length is a compile-time constant.  A block in column j has len[j] / NP species
+// sub-blocks of NP columns, each streamed with the fully unrolled chunk loop of the uniform kernel (V divides NP,
+// so no chunk straddles a species boundary and there is no scalar tail).
+template <typename T, int NP, int NS, int V, int MODE>
+__device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, const int32_t* __restrict__ rows,
+                                           const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                           const int32_t* __restrict__ len, const int64_t* __restrict__ i0,
+                                           const int64_t* __restrict__ boff, const T* __restrict__ vals,
+                                           const T* __restrict__ x, const T* __restrict__ z, T* __restrict__ y,
+                                           T alpha, T beta, const T* __restrict__ dinv,
+                                           const int64_t* __restrict__ doff) {
+  constexpr int I = NP * NS;
+  static_assert(NP % V == 0, "chunk width must divide the species block");
+  const int t = threadIdx.x;
+  const int lb = t / I;
+  const int r = t - lb * I;
+  const int64_t b = b0 + lb;
+  const bool valid = (lb < BPC) && (b < nrows);
+  const int64_t i = valid ? rows[b] : 0;
+  const uint64_t pol = policy_evict_first();
+  T acc0 = 0, acc1 = 0;
+  if (valid) {
+    const int64_t k0 = rp[i], k1 = rp[i + 1];
+    for (int64_t k = k0; k < k1; ++k) {
+      const int64_t j = ci[k];
+      const int sj = len[j] / NP;
+      const T* vb = vals + boff[k] + r * V;
+      const T* xb = x + i0[j];
+      for (int sp = 0; sp < sj; ++sp) {
+#pragma unroll
+        for (int c = 0; c < NP / V; ++c) {
+          const int col = sp * NP + c * V;
+          Vec<T, V> a = ldv_stream<T, V>(vb + (int64_t)(col / V) * (I * V), pol);
+          Vec<T, V> xv = ldv_cached<T, V>(xb + col);
+#pragma unroll
+          for (int q = 0; q < V; ++q) {
+            if ((c * V + q) & 1)
+              acc1 = fma(a.a[q], xv.a[q], acc1);
+            else
+              acc0 = fma(a.a[q], xv.a[q], acc0);
+          }
+        }
+      }
+    }
+  }
+  const T acc = acc0 + acc1;
+  const int64_t g = valid ? i0[i] + r : 0;
+  if constexpr (MODE == 0) {
+    if (valid) {
+      T out = alpha * acc;
+      if (z != nullptr) out = fma(beta, z[g], out);
+      y[g] = out;
+    }
+  } else {
+    __shared__ T q[256];
+    q[t] = valid ? (z[g] - acc) : T(0);
+    __syncthreads();
+    if (valid) {
+      const T* D = dinv + doff[i] + r;
+      const T* qb = q + lb * I;
+      T s0 = 0, s1 = 0;
+#pragma unroll
+      for (int c = 0; c < I; c += 2) {
+        s0 = fma(D[c * I], qb[c], s0);
+        if (c + 1 < I) s1 = fma(D[(c + 1) * I], qb[c + 1], s1);
+      }
+      y[g] = fma(alpha, s0 + s1, x[g]);
+    }
+  }
+}
+
+// One launch for both species counts: CTAs [0, cta1) take the one-species rows, the rest the two-species rows.
+template <typename T, int NP, int V, int MODE>
+__global__ void __launch_bounds__(256) spmv_typed_kernel(
+    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const int32_t* __restrict__ len,
+    const int64_t* __restrict__ i0, const int64_t* __restrict__ boff, const int32_t* __restrict__ rows,
+    int64_t n1, int64_t n2, int64_t cta1, const T* __restrict__ vals, const T* __restrict__ x,
+    const T* __restrict__ z, T* __restrict__ y, T alpha, T beta, const T* __restrict__ dinv,
+    const int64_t* __restrict__ doff, const int* __restrict__ active) {
+  if (active != nullptr && *active == 0) return;
+  const int bpc1 = blockDim.x / NP, bpc2 = blockDim.x / (2 * NP);
+  if ((int64_t)blockIdx.x < cta1)
+    typed_rows<T, NP, 1, V, MODE>(bpc1, (int64_t)blockIdx.x * bpc1, n1, rows, rp, ci, len, i0, boff, vals, x, z, y,
+                                  alpha, beta, dinv, doff);
+  else
+    typed_rows<T, NP, 2, V, MODE>(bpc2, ((int64_t)blockIdx.x - cta1) * bpc2, n2, rows + n1, rp, ci, len, i0, boff,
+                                  vals, x, z, y, alpha, beta, dinv, doff);
+}
+
 // y = alpha * Dinv * b (block diagonal, column-major blocks)
 template <typename T>
 __global__ void blockdiag_kernel(const int32_t* __restrict__ len, const int64_t* __restrict__ i0,
@@ -313,6 +407,25 @@ void finish_structure(Matrix& M) {
   for (int64_t i = 0; i < M.nb; ++i) dof[i + 1] = dof[i] + (int64_t)M.h_len[i] * M.h_len[i];
   M.doff.alloc(M.nb + 1);
   BSGPU_CUDA(cudaMemcpy(M.doff.p, dof.data(), (M.nb + 1) * 8, cudaMemcpyHostToDevice));
+  // species-count groups for the typed kernels (one or two species of Np modes, Np in {1, 4, 10, 20})
+  M.typed = false;
+  M.grp_n1 = M.grp_n2 = 0;
+  bool two_at_most = M.nb > 0;
+  for (int64_t i = 0; i < M.nb && two_at_most; ++i) two_at_most = M.h_len[i] == M.Np || M.h_len[i] == 2 * M.Np;
+  const bool np_ok = M.Np == 1 || M.Np == 4 || M.Np == 10 || M.Np == 20;
+  if (!M.uniform && two_at_most && np_ok && M.Np % M.V == 0) {
+    std::vector<int32_t> g;
+    g.reserve(M.nb);
+    for (int64_t i = 0; i < M.nb; ++i)
+      if (M.h_len[i] == M.Np) g.push_back((int32_t)i);
+    M.grp_n1 = (int64_t)g.size();
+    for (int64_t i = 0; i < M.nb; ++i)
+      if (M.h_len[i] == 2 * M.Np) g.push_back((int32_t)i);
+    M.grp_n2 = (int64_t)g.size() - M.grp_n1;
+    M.grp_rows.alloc(g.size());
+    BSGPU_CUDA(cudaMemcpy(M.grp_rows.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    M.typed = true;
+  }
   M.row2blk.alloc(std::max<int64_t>(M.N, 1));
   M.cta_row0.alloc(packs.size());
   if (M.N) BSGPU_CUDA(cudaMemcpy(M.row2blk.p, r2b.data(), M.N * 4, cudaMemcpyHostToDevice));
@@ -348,7 +461,7 @@ bool specialised(const Matrix& A) {
 template <typename T, int NP, int V, int MODE>
 void launch_uniform(const Matrix& A, const T* vals, const T* x, const T* z, T* y, T alpha, T beta, const T* dinv,
                     cudaStream_t st, const int* active) {
-  constexpr int BPC = 256 / NP;
+  const int BPC = std::max(1, A.cta[MODE == 1 ? 1 : 0] / NP);
   const int64_t grid = (A.nb + BPC - 1) / BPC;
   if (grid == 0) return;
   spmv_uniform_kernel<T, NP, V, MODE><<<(unsigned)grid, BPC * NP, 0, st>>>(A.rp.p, A.ci.p, vals, x, z, y, alpha, beta,
@@ -366,9 +479,45 @@ void launch_general(const Matrix& A, const T* vals, const T* x, const T* z, T* y
   BSGPU_CHECK_LAUNCH();
 }
 
+template <typename T, int NP, int V, int MODE>
+void launch_typed(const Matrix& A, const T* vals, const T* x, const T* z, T* y, T alpha, T beta, const T* dinv,
+                  const int64_t* doff, cudaStream_t st, const int* active) {
+  const int threads = std::max(A.cta[MODE == 1 ? 1 : 0], 2 * NP);
+  const int64_t bpc1 = threads / NP, bpc2 = threads / (2 * NP);
+  const int64_t cta1 = (A.grp_n1 + bpc1 - 1) / bpc1, cta2 = (A.grp_n2 + bpc2 - 1) / bpc2;
+  if (cta1 + cta2 == 0) return;
+  spmv_typed_kernel<T, NP, V, MODE><<<(unsigned)(cta1 + cta2), threads, 0, st>>>(
+      A.rp.p, A.ci.p, A.len.p, A.i0.p, A.boff.p, A.grp_rows.p, A.grp_n1, A.grp_n2, cta1, vals, x, z, y, alpha, beta,
+      dinv, doff, active);
+  BSGPU_CHECK_LAUNCH();
+}
+
+// the (Np, V) pairs of the typed kernels; false: not covered (the general kernel serves the matrix)
+template <typename T, int MODE>
+bool dispatch_typed(const Matrix& A, const T* vals, const T* x, const T* z, T* y, T alpha, T beta, const T* dinv,
+                    const int64_t* doff, cudaStream_t st, const int* active) {
+  if (!A.typed) return false;
+#define BSGPU_TYPED(NP, VV)                                                                       \
+  if (A.Np == NP && A.V == VV) {                                                                  \
+    launch_typed<T, NP, VV, MODE>(A, vals, x, z, y, alpha, beta, dinv, doff, st, active);         \
+    return true;                                                                                  \
+  }
+  BSGPU_TYPED(1, 1)
+  BSGPU_TYPED(4, 2)
+  BSGPU_TYPED(10, 2)
+  BSGPU_TYPED(20, 2)
+  if constexpr (sizeof(T) == 4) {
+    BSGPU_TYPED(4, 4)
+    BSGPU_TYPED(20, 4)
+  }
+#undef BSGPU_TYPED
+  return false;
+}
+
 template <typename T, int MODE>
 void dispatch(const Matrix& A, const T* vals, const T* x, const T* z, T* y, T alpha, T beta, const T* dinv,
               const int64_t* doff, cudaStream_t st, const int* active) {
+  if (dispatch_typed<T, MODE>(A, vals, x, z, y, alpha, beta, dinv, doff, st, active)) return;
   if (specialised(A)) {
     constexpr int VW = sizeof(T) == 8 ? 2 : 4;
     switch (A.Np) {
@@ -648,6 +797,111 @@ void blockdiag_apply(const Matrix& A, const double* dinv, double omega, const do
 void blockdiag_apply(const Matrix& A, const float* dinv, float omega, const float* b, float* y, cudaStream_t st,
                      const int* active) {
   blockdiag_impl<float>(A, dinv, omega, b, y, st, active);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// autotuner of the launch shape
+// ---------------------------------------------------------------------------------------------------------------
+namespace {
+
+std::mutex g_tune_mutex;
+std::map<std::string, int> g_tune_cache;
+std::vector<std::string> g_tune_log;
+
+template <typename T>
+float time_launches(const Matrix& A, int mode, const T* dinv, const T* x, const T* b, T* y, cudaStream_t st, int reps) {
+  cudaEvent_t e0, e1;
+  BSGPU_CUDA(cudaEventCreate(&e0));
+  BSGPU_CUDA(cudaEventCreate(&e1));
+  const T* vals = A.single ? (const T*)(const void*)A.v32.p : (const T*)(const void*)A.v64.p;
+  auto one = [&]() {
+    if (mode == 0)
+      dispatch<T, 0>(A, vals, x, nullptr, y, T(1), T(0), nullptr, nullptr, st, nullptr);
+    else
+      dispatch<T, 1>(A, vals, x, b, y, T(1), T(0), dinv, A.doff.p, st, nullptr);
+  };
+  for (int i = 0; i < 2; ++i) one();
+  BSGPU_CUDA(cudaEventRecord(e0, st));
+  for (int i = 0; i < reps; ++i) one();
+  BSGPU_CUDA(cudaEventRecord(e1, st));
+  BSGPU_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  BSGPU_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / reps;
+}
+
+template <typename T>
+void autotune_impl(const Matrix& A, int mode, const T* dinv, cudaStream_t st) {
+  const bool tunable = A.typed || specialised(A);
+  if (!tunable || A.tuned[mode] || A.N == 0) return;
+  int dev = 0;
+  BSGPU_CUDA(cudaGetDevice(&dev));
+  std::ostringstream key;
+  key << dev << (A.typed ? ":typed:" : ":uniform:") << (A.single ? "f32" : "f64") << ":Np" << A.Np << ":V" << A.V
+      << ":mode" << mode << ":nb" << A.nb << ":nnzb" << A.nnzb << ":N" << A.N;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key.str());
+    if (it != g_tune_cache.end()) {
+      A.cta[mode] = it->second;
+      A.tuned[mode] = true;
+      return;
+    }
+  }
+  // launches costing about 2 ms in total per candidate, at least 5
+  const double bytes = (double)A.value_bytes() + 3.0 * (double)A.N * sizeof(T);
+  const int reps = (int)std::max(5.0, std::min(200.0, 2e-3 / (bytes / 5e12)));
+  DBuf<T> x(A.N), b(A.N), y(A.N);
+  BSGPU_CUDA(cudaMemsetAsync(x.p, 0, A.N * sizeof(T), st));
+  BSGPU_CUDA(cudaMemsetAsync(b.p, 0, A.N * sizeof(T), st));
+  const int cands[3] = {256, 128, 64};
+  const int saved = A.cta[mode];
+  std::ostringstream rec;
+  rec << "{\"matrix\": \"" << key.str() << "\", \"times_ms\": {";
+  int best = 256;
+  float tbest = 1e30f;
+  for (int ci = 0; ci < 3; ++ci) {
+    const int c = cands[ci];
+    if (!A.typed && c < A.Np) continue;
+    if (A.typed && c < 2 * A.Np) continue;
+    A.cta[mode] = c;
+    const float t = time_launches<T>(A, mode, dinv, x.p, b.p, y.p, st, reps);
+    rec << (ci ? ", " : "") << "\"" << c << "\": " << t;
+    if (t < tbest) {
+      tbest = t;
+      best = c;
+    }
+  }
+  (void)saved;
+  A.cta[mode] = best;
+  A.tuned[mode] = true;
+  rec << "}, \"threads_per_cta\": " << best << ", \"reps\": " << reps << "}";
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tune_cache[key.str()] = best;
+  g_tune_log.push_back(rec.str());
+}
+
+}  // namespace
+
+void autotune(const Matrix& A, int mode, const void* dinv, cudaStream_t st) {
+  require(mode == 0 || mode == 1, "autotune: mode 0 (product) or 1 (block-Jacobi update)");
+  require(mode == 0 || dinv != nullptr, "autotune: the block-Jacobi update needs the factors");
+  cudaStreamCaptureStatus cs;
+  BSGPU_CUDA(cudaStreamIsCapturing(st, &cs));
+  require(cs == cudaStreamCaptureStatusNone, "autotune inside a graph capture");
+  if (A.single)
+    autotune_impl<float>(A, mode, (const float*)dinv, st);
+  else
+    autotune_impl<double>(A, mode, (const double*)dinv, st);
+}
+
+std::string autotune_report() {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  std::string out = "[";
+  for (size_t i = 0; i < g_tune_log.size(); ++i) out += (i ? ", " : "") + g_tune_log[i];
+  return out + "]";
 }
 
 }  // namespace bsgpu

@@ -28,6 +28,16 @@ struct Matrix {
   DBuf<int64_t> doff;      // offsets of the per-block-row diagonal factors (I*I each)
   DBuf<int64_t> cta_row0;  // CTA packing for the variable-size kernels (whole block rows per CTA)
   int64_t ncta = 0;
+  // Blocks of one or two species (XDG): the block rows with one species, then those with two, each list in
+  // ascending order; the typed kernels specialise on the species count of the row (typed == false: the general
+  // kernel with per-row lookups serves the matrix).
+  bool typed = false;
+  DBuf<int32_t> grp_rows;
+  int64_t grp_n1 = 0, grp_n2 = 0;
+  // Launch shape of the uniform and species-count kernels: threads per CTA (whole block rows each) for the plain
+  // product (cta[0]) and the fused block-Jacobi update (cta[1]); 256 unless the autotuner picked otherwise.
+  mutable int cta[2] = {256, 256};
+  mutable bool tuned[2] = {false, false};
   int cta_threads = 256;
   DBuf<double> v64;
   DBuf<float> v32;
@@ -73,5 +83,12 @@ void blockdiag_apply(const Matrix& A, const float* dinv, float omega, const floa
 
 // Offsets of the per-block-row dense diagonal factors (column-major I x I each) and their total size.
 std::vector<int64_t> diag_offsets(const Matrix& A);
+
+// Autotuner of the launch shape (threads per CTA: 256, 128 or 64, whole block rows per CTA) of the product
+// (mode 0) or of the fused block-Jacobi update (mode 1, with the factors dinv of the matrix's precision) on the
+// matrix itself: every candidate is timed with CUDA events and the fastest is kept in A.cta.  Results are cached
+// per device and matrix shape and recorded for autotune_report.  Not during a graph capture.
+void autotune(const Matrix& A, int mode, const void* dinv, cudaStream_t st);
+std::string autotune_report();
 
 }  // namespace bsgpu

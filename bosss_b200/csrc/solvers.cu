@@ -23,7 +23,135 @@ Ctx::Ctx() {
 }
 Ctx::~Ctx() {
   if (hscal) cudaFreeHost(hscal);
+  if (h_err) cudaFreeHost(h_err);
+  for (cudaStream_t b : body_streams) cudaStreamDestroy(b);
   if (st) cudaStreamDestroy(st);
+}
+
+namespace {
+constexpr int kMaxBodies = 8192;
+constexpr int kMaxDepth = 16;
+}  // namespace
+
+void Ctx::graph_init() {
+  if (h_err) return;
+  d_err = flag();
+  BSGPU_CUDA(cudaMallocHost(&h_err, sizeof(int)));
+  *h_err = 0;
+  d_exec.alloc(kMaxBodies);
+  BSGPU_CUDA(cudaMemset(d_exec.p, 0, kMaxBodies * sizeof(unsigned int)));
+  h_exec.assign(kMaxBodies, 0);
+  for (int i = 0; i < kMaxDepth; ++i) {
+    cudaStream_t b = nullptr;
+    BSGPU_CUDA(cudaStreamCreateWithFlags(&b, cudaStreamNonBlocking));
+    body_streams.push_back(b);
+  }
+}
+
+void Ctx::capture_begin() {
+  graph_init();
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  body_kernels.assign(1, 0);
+  body_stack.clear();
+  st_stack.clear();
+  cur_body = 0;
+  BSGPU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+  capturing = true;
+  mark = launches_now();
+}
+
+long long Ctx::capture_end(cudaGraph_t* g) {
+  require(st_stack.empty(), "graph capture: unbalanced conditional bodies");
+  body_kernels[cur_body] += (long long)(launches_now() - mark);
+  capturing = false;
+  BSGPU_CUDA(cudaStreamEndCapture(st, g));
+  long long total = 0;
+  for (long long k : body_kernels) total += k;
+  add_launches(-total);  // recorded, not launched: replays add what they run
+  return body_kernels[0];
+}
+
+int Ctx::new_body() {
+  require(capturing, "conditional body outside a graph capture");
+  require((int)body_kernels.size() < kMaxBodies, "graph capture: too many conditional bodies",
+          BSGPU_ERR_UNSUPPORTED);
+  body_kernels.push_back(0);
+  return (int)body_kernels.size() - 1;
+}
+
+cudaGraphConditionalHandle Ctx::cond_handle() {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  BSGPU_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+  require(cs == cudaStreamCaptureStatusActive, "conditional handle outside a graph capture");
+  cudaGraphConditionalHandle h;
+  BSGPU_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+  return h;
+}
+
+void Ctx::cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, int body) {
+  require((int)st_stack.size() < kMaxDepth, "graph capture: conditional bodies nested too deeply",
+          BSGPU_ERR_UNSUPPORTED);
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  BSGPU_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &ndeps));
+  require(cs == cudaStreamCaptureStatusActive, "conditional node outside a graph capture");
+  cudaGraphNodeParams p{};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = h;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  BSGPU_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &p));
+  cudaGraph_t body_graph = p.conditional.phGraph_out[0];
+  BSGPU_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  body_kernels[cur_body] += (long long)(launches_now() - mark);
+  body_stack.push_back(cur_body);
+  cur_body = body;
+  st_stack.push_back(st);
+  st = body_streams[st_stack.size() - 1];
+  BSGPU_CUDA(cudaStreamBeginCaptureToGraph(st, body_graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  mark = launches_now();
+}
+
+void Ctx::cond_end() {
+  require(!st_stack.empty(), "graph capture: no open conditional body");
+  body_kernels[cur_body] += (long long)(launches_now() - mark);
+  cudaGraph_t g = nullptr;
+  BSGPU_CUDA(cudaStreamEndCapture(st, &g));
+  st = st_stack.back();
+  st_stack.pop_back();
+  cur_body = body_stack.back();
+  body_stack.pop_back();
+  mark = launches_now();
+}
+
+void Ctx::check_graph_errors() {
+  if (!err_pending) return;
+  err_pending = false;
+  const int e = *h_err;
+  if (e == 0) return;
+  *h_err = 0;
+  BSGPU_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  if (e & kDevErrSlots) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: history slots exhausted");
+  if (e & kDevErrResidualIncrease) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: residual increase");
+  throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: NaN/Inf in the preconditioner");
+}
+
+void Ctx::flush_graph_counts() {
+  if (!graph_ran) return;
+  graph_ran = false;
+  const size_t nb = body_kernels.size();
+  BSGPU_CUDA(cudaMemcpyAsync(h_exec.data(), d_exec.p, nb * sizeof(unsigned int), cudaMemcpyDeviceToHost, st));
+  BSGPU_CUDA(cudaMemsetAsync(d_exec.p, 0, nb * sizeof(unsigned int), st));
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  long long n = 0;
+  for (size_t b = 1; b < nb; ++b) n += body_kernels[b] * (long long)h_exec[b];
+  add_launches(n);
+  check_graph_errors();
 }
 double* Ctx::scal(int n) {
   require(nscal + n <= scal_cap, "solver tree needs too many device scalars", BSGPU_ERR_UNSUPPORTED);
@@ -36,8 +164,10 @@ int* Ctx::flag() {
   return dflag.p + nflag++;
 }
 void Ctx::fetch(const double* d, int n) {
+  require(!capturing, "host read of a device scalar inside a graph capture");
   BSGPU_CUDA(cudaMemcpyAsync(hscal + (d - dscal.p), d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
   BSGPU_CUDA(cudaStreamSynchronize(st));
+  check_graph_errors();
 }
 void Ctx::check_flag(const int* f, const char* what) {
   int h = 0;
@@ -110,6 +240,7 @@ int elt_grid(int64_t n) {
 // ---------------------------------------------------------------------------------------------------------------
 template <typename T>
 struct BlockJacobiT : Solver<T> {
+  bool graphable() const override { return true; }
   const Matrix* A;
   DBuf<T> dinv;
   DBuf<T> tmp;
@@ -126,6 +257,8 @@ struct BlockJacobiT : Solver<T> {
       invert_diag_blocks(*A64, nullptr, dinv.p, err, c.st);
     c.check_flag(err, "BlockJacobi: singular diagonal block");
     tmp.alloc(std::max<int64_t>(A->N, 1));
+    c.tune(*A, 1, dinv.p);
+    c.tune(*A, 0);
   }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
     TraceScope ts(c, this->trace);
@@ -154,6 +287,7 @@ struct BlockJacobiT : Solver<T> {
 // smoothing BoSSS uses on its low p-levels (CellILU, PmgConfig.cs:124-141).
 template <typename T>
 struct BlockGST : Solver<T> {
+  bool graphable() const override { return true; }
   const Matrix* A;
   DBuf<T> dinv;
   std::vector<DBuf<int32_t>> rows;
@@ -198,6 +332,7 @@ struct BlockGST : Solver<T> {
 // for the mixed-precision preconditioner.
 template <typename T>
 struct ILU0T : Solver<T> {
+  bool graphable() const override { return true; }
   std::unique_ptr<Matrix> M64, M32;
   const Matrix* M = nullptr;
   DBuf<T> uinv;
@@ -256,6 +391,7 @@ struct ILU0T : Solver<T> {
 // for BlockJacobi.
 template <typename T>
 struct SchwarzT : Solver<T> {
+  bool graphable() const override { return true; }
   const Matrix* A;
   std::unique_ptr<Matrix> M;
   DBuf<T> r;
@@ -266,6 +402,8 @@ struct SchwarzT : Solver<T> {
     schwarz_factor(*A64, *M, err, c.st);
     c.check_flag(err, "Schwarz: singular block");
     r.alloc(std::max<int64_t>(A->N, 1));
+    c.tune(*A, 0);
+    c.tune(*M, 0);
   }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
     TraceScope ts(c, this->trace);
@@ -347,6 +485,7 @@ struct PCGT : Solver<T> {
         invert_diag_blocks(*A64, nullptr, dinv.p, err, c.st);
       c.check_flag(err, "PCG: singular diagonal block");
     }
+    c.tune(*A, 0);
   }
   void apply_pc(Ctx& c, const T* in, T* out, const int* act) {
     if (precond)
@@ -457,6 +596,60 @@ struct PCGT : Solver<T> {
     }
     this->this_level_iterations = it;
     if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += it;
+  }
+  bool graphable() const override { return term.max_iter <= kMaxRecordedIterations && term.min_iter <= term.max_iter; }
+  // Recorded form: the initialisation, then a WHILE node whose body is one CG iteration; the fused update's
+  // termination step clears `active` (at the latest when the iteration count passes max_iter), which ends the loop.
+  void solve_graph(Ctx& c, T* X, const T* B, bool zero) override {
+    require(graphable(), "coarse CG: iteration limits cannot be recorded");
+    const int64_t N = A->N;
+    if (zero)
+      copy_vec(r.p, B, N, c.st);
+    else
+      spmv(*A, T(-1), X, T(1), B, r.p, c.st);
+    apply_pc(c, r.p, z.p, nullptr);
+    copy_vec(p.p, z.p, N, c.st);
+    {
+      const T* a[2] = {r.p, r.p};
+      const T* b[2] = {z.p, r.p};
+      dots(c.red, 2, a, b, N, s + 2, 0, c.st);
+    }
+    pcg_init_kernel<<<1, 1, 0, c.st>>>(s, active);
+    BSGPU_CHECK_LAUNCH();
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body();
+    cond_set(h, active, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeWhile, body);
+    iteration_kernels(c, X);
+    cond_set(h, active, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_end();
+  }
+  // one CG iteration on c.st, every kernel predicated on `active`
+  void iteration_kernels(Ctx& c, T* X) {
+    const int64_t N = A->N;
+    const int grid = elt_grid(N);
+    const bool fused = precond && A->uniform && A->nb > 0 && (A->Np == 4 || A->Np == 6 || A->Np == 10 || A->Np == 20);
+    const T* px[1] = {p.p};
+    const T* qx[1] = {q.p};
+    spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, c.st, active);
+    dots(c.red, 1, px, qx, N, s + 1, 0, c.st, active);
+    if (fused) {
+      pcg_update(c.red, A->Np, s, active, X, p.p, q.p, r.p, z.p, dinv.p, A->nb, term.mode, term.tol, term.max_iter,
+                 term.min_iter, c.st);
+    } else {
+      pcg_alpha_kernel<<<1, 1, 0, c.st>>>(s, active);
+      BSGPU_CHECK_LAUNCH();
+      axpys(1, s + 7, nullptr, 1.0, px, X, N, c.st, active);
+      axpys(1, s + 7, nullptr, -1.0, qx, r.p, N, c.st, active);
+      apply_pc(c, r.p, z.p, active);
+      const T* a[2] = {r.p, r.p};
+      const T* b[2] = {z.p, r.p};
+      dots(c.red, 2, a, b, N, s + 2, 0, c.st, active);
+      pcg_beta_kernel<<<1, 1, 0, c.st>>>(s, active, term.mode, term.tol, term.max_iter, term.min_iter);
+      BSGPU_CHECK_LAUNCH();
+    }
+    xpby_kernel<T><<<grid, 256, 0, c.st>>>(z.p, s + 6, p.p, N, active);
+    BSGPU_CHECK_LAUNCH();
   }
 };
 
@@ -658,6 +851,87 @@ struct OrthoT {
     if (rn > oldN + tol) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: residual increase");
     return rn;
   }
+
+  // ---- recorded form (graph capture): the history length lives on the device ----------------------------------
+  // A new correction is built in the fixed buffers W (correction) and MW (its image), projected against the
+  // history by the device-count kernels, normalised and copied into history slot k; MinimizeResidual then uses
+  // W and MW.  A correction with nothing independent of the history left is stored as zero (devctl.cu).
+  int nslots = 0;
+  DBuf<T> W, MW;
+  DBuf<T*> d_sol, d_mxx;
+  DBuf<OrthoState> state;
+  HistScratch hs;
+  double* d_hbeta = nullptr;  // projection coefficients of the recorded form [nslots]
+  double* d_rn = nullptr;     // residual norm after MinimizeResidual
+  OrthoState* dev() { return state.p; }
+  void prepare_dev(Ctx& c, int slots) {
+    slots = std::max(1, std::min(slots, cap));
+    require(slots <= kHistMax, "recorded OrthoMG: history longer than 128", BSGPU_ERR_UNSUPPORTED);
+    if (nslots >= slots) return;
+    while ((int)Sol.size() < slots) {
+      Sol.emplace_back(std::max<int64_t>(N, 1));
+      Mxx.emplace_back(std::max<int64_t>(N, 1));
+    }
+    W.alloc(std::max<int64_t>(N, 1));
+    MW.alloc(std::max<int64_t>(N, 1));
+    std::vector<T*> ps(slots), pm(slots);
+    for (int j = 0; j < slots; ++j) {
+      ps[j] = Sol[j].p;
+      pm[j] = Mxx[j].p;
+    }
+    d_sol.alloc(slots);
+    d_mxx.alloc(slots);
+    BSGPU_CUDA(cudaMemcpy(d_sol.p, ps.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
+    BSGPU_CUDA(cudaMemcpy(d_mxx.p, pm.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
+    if (!state.p) {
+      state.alloc(1);
+      BSGPU_CUDA(cudaMemset(state.p, 0, sizeof(OrthoState)));
+      d_rn = c.scal(1);
+    }
+    hs.init(slots);
+    d_hbeta = c.scal(slots);
+    nslots = slots;
+  }
+  T* next_sol_dev(Ctx& c) {
+    fill(T(0), W.p, N, c.st);
+    return W.p;
+  }
+  // one projection sweep of (W, MW) against the first k history entries; |MW| after it into d_proj[0] and, with
+  // `self`, |MW|^2 before it into d_proj[1]
+  void cgs_dev(Ctx& c, bool self) {
+    hist_dots(hs, d_mxx.p, &state.p->k, MW.p, N, d_hbeta, self ? d_proj + 1 : nullptr, c.st);
+    hist_axpy2(d_sol.p, d_mxx.p, &state.p->k, nslots, d_hbeta, W.p, MW.p, N, c.st);
+    const T* a[1] = {MW.p};
+    dots(c.red, 1, a, a, N, d_proj, 1, c.st);
+  }
+  void add_sol_dev(Ctx& c) {
+    spmv(*A, T(1), W.p, T(0), (const T*)nullptr, MW.p, c.st);
+    cgs_dev(c, true);
+    ortho_decide1(state.p, d_proj, c.d_err, c.st);
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body();
+    cond_set(h, &state.p->second, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeIf, body);
+    cgs_dev(c, false);
+    ortho_decide2(state.p, d_proj, c.st);
+    c.cond_end();
+    ortho_final(state.p, d_proj, c.st);
+    ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
+    ortho_advance(state.p, recalc_period, nslots, c.st);
+  }
+  void minimize_dev(Ctx& c, T* X, const T* B, const T* Res0, T* Res, const TermParams& tp) {
+    const T* a[1] = {MW.p};
+    const T* b[1] = {Res0};
+    dots(c.red, 1, a, b, N, d_alpha, 0, c.st);
+    const T* sx[1] = {W.p};
+    axpys(1, d_alpha, nullptr, 1.0, sx, X, N, c.st);
+    spmv(*A, T(-1), X, T(1), B, Res, c.st, &state.p->recalc);
+    const T* mx[1] = {MW.p};
+    axpys(1, d_alpha, nullptr, -1.0, mx, Res, N, c.st, &state.p->update);
+    const T* r[1] = {Res};
+    dots(c.red, 1, r, r, N, d_rn, 1, c.st);
+    minimize_check(state.p, d_rn, tp, c.d_err, c.st);
+  }
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -755,6 +1029,88 @@ struct OrthoMGT : Solver<T> {
       if (c.tracing && this->trace >= 0) c.trace[this->trace].iterations += 1;
     }
   }
+
+  // ---- recorded form --------------------------------------------------------------------------------------------
+  // The loop above with its decisions on the device: iterations in a WHILE node (inline for a fixed single
+  // iteration, the p-multigrid preconditioner's top level), each correction after the first of an iteration in an
+  // IF node on (level active, no cancellation, history not full).
+  bool graphable() const override {
+    return (!coarse || coarse->graphable()) && (!post || post->graphable()) && (!pre || pre->graphable()) &&
+           ortho.cap <= kHistMax;
+  }
+  int corrections_per_iteration() const {
+    return (coarse ? 1 : 0) + (post ? sweeps : 0) + ((pre && (pre_on == nullptr || *pre_on)) ? 1 : 0);
+  }
+  void prepare_graph(Ctx& c) override {
+    const int per = std::max(1, corrections_per_iteration());
+    const long long most = (long long)std::max(1, term.max_iter) * per;
+    ortho.prepare_dev(c, (int)std::min<long long>(most, ortho.cap));
+    if (coarse) coarse->prepare_graph(c);
+    if (post) post->prepare_graph(c);
+    if (pre) pre->prepare_graph(c);
+  }
+  void correction_dev(Ctx& c, Solver<T>* sv, T* X, const T* B, const TermParams& tp) {
+    T* w = ortho.next_sol_dev(c);
+    sv->solve_graph(c, w, Res.p, true);
+    ortho.add_sol_dev(c);
+    ortho.minimize_dev(c, X, B, Res0.p, Res.p, tp);
+  }
+  // a correction recorded inside an IF node on (active && !cancel && k < cap) (post-smoother sweeps) or on
+  // `active` alone
+  void guarded_correction_dev(Ctx& c, Solver<T>* sv, T* X, const T* B, const TermParams& tp, bool post_sweep,
+                              int cap_eff) {
+    OrthoState* st = ortho.dev();
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body();
+    cond_set(h, &st->active, post_sweep ? &st->cancel : nullptr, post_sweep ? &st->k : nullptr, cap_eff,
+             c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeIf, body);
+    correction_dev(c, sv, X, B, tp);
+    c.cond_end();
+  }
+  void iteration_dev(Ctx& c, T* X, const T* B, const TermParams& tp) {
+    OrthoState* st = ortho.dev();
+    const int cap_eff = ortho.nslots;
+    iter_begin(st, cap_eff, c.st);
+    copy_if(Res.p, Res0.p, N, &st->restart, c.st);
+    bool first = true;
+    auto run = [&](Solver<T>* sv, bool post_sweep) {
+      if (first)
+        correction_dev(c, sv, X, B, tp);
+      else
+        guarded_correction_dev(c, sv, X, B, tp, post_sweep, cap_eff);
+      first = false;
+    };
+    if (pre && (pre_on == nullptr || *pre_on)) run(pre.get(), false);
+    if (coarse) run(coarse.get(), false);
+    if (post)
+      for (int g = 0; g < sweeps; ++g) run(post.get(), true);
+  }
+  void solve_graph(Ctx& c, T* X, const T* B, bool zero) override {
+    if (zero)
+      copy_vec(Res0.p, B, N, c.st);
+    else
+      spmv(*A, T(-1), X, T(1), B, Res0.p, c.st);
+    copy_vec(Res.p, Res0.p, N, c.st);
+    const T* a[1] = {Res0.p};
+    dots(c.red, 1, a, a, N, ortho.d_norm, 1, c.st);
+    const TermParams tp = term.params();
+    OrthoState* st = ortho.dev();
+    level_begin(st, ortho.d_norm, tp, c.st);
+    if (term.mode == 2 && term.max_iter == 1) {
+      iteration_dev(c, X, B, tp);
+      iter_end(st, tp, c.st);
+      return;
+    }
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body();
+    cond_set(h, &st->active, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeWhile, body);
+    iteration_dev(c, X, B, tp);
+    iter_end(st, tp, c.st);
+    cond_set(h, &st->active, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_end();
+  }
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -799,6 +1155,30 @@ struct GridAndDegT : Solver<T> {
     lower->solve(c, xLo.p, bLo.p, zero);
     this->converged = lower->converged;
     restrict_scatter_add(xLo.p, X, sub->N, A->Np, keep, map.p, c.st);
+  }
+  // recorded form: the zero-right-hand-side return becomes an IF node on |b_lo| > 0
+  int* nonzero = nullptr;
+  bool graphable() const override { return lower && lower->graphable(); }
+  void prepare_graph(Ctx& c) override {
+    if (!nonzero) nonzero = c.flag();
+    lower->prepare_graph(c);
+  }
+  void solve_graph(Ctx& c, T* X, const T* B, bool zero) override {
+    restrict_gather(B, bLo.p, sub->N, A->Np, keep, map.p, c.st);
+    const T* a[1] = {bLo.p};
+    dots(c.red, 1, a, a, sub->N, d_norm, 1, c.st);
+    positive_flag(d_norm, nonzero, c.st);
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body();
+    cond_set(h, nonzero, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeIf, body);
+    if (zero)
+      fill(T(0), xLo.p, sub->N, c.st);
+    else
+      restrict_gather(X, xLo.p, sub->N, A->Np, keep, map.p, c.st);
+    lower->solve_graph(c, xLo.p, bLo.p, zero);
+    restrict_scatter_add(xLo.p, X, sub->N, A->Np, keep, map.p, c.st);
+    c.cond_end();
   }
 };
 
@@ -1032,6 +1412,7 @@ struct AmgPcgT : Solver<T> {
 // The learned stage as a preconditioner / smoother: X = NN(B) (learned.cu); inputs normalised by the RMS of B.
 template <typename T>
 struct LearnedPrecondT : Solver<T> {
+  bool graphable() const override { return true; }
   const LearnedNet* net;
   int64_t N;
   double* d_s;  // [0] |B|, [1] scale
@@ -1068,6 +1449,88 @@ struct MixedAdapter : Solver<double> {
     convert(x32.p, X, N, c.st);
     this->converged = inner->converged;
     this->this_level_iterations = inner->this_level_iterations;
+  }
+};
+
+// The p-multigrid V-cycle recorded once as a CUDA graph (device-side control flow, devctl.cuh) and replayed by one
+// graph launch per application.  The graph reads and writes fixed buffers: the owner's (MixedAdapter's FP32
+// vectors, which it fills before and reads after the call) or this wrapper's own (the right-hand side is copied in,
+// the result out).  Recorded again when the learned pre-smoother is switched on or off.
+template <typename T>
+struct GraphedT : Solver<T> {
+  std::unique_ptr<Solver<T>> inner;
+  int64_t N;
+  T* Xs = nullptr;          // owner's buffers (X is zero on entry), or null: own buffers
+  const T* Bs = nullptr;
+  DBuf<T> xin, bin;
+  const bool* key_src = nullptr;
+  int key = -1;
+  cudaGraphExec_t exec = nullptr;
+  long long top_kernels = 0;
+  GraphedT(int64_t n, std::unique_ptr<Solver<T>> in) : inner(std::move(in)), N(n) {}
+  ~GraphedT() override {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+  int nested() const override { return inner->this_level_iterations + inner->nested(); }
+  void capture(Ctx& c, T* X, const T* B) {
+    if (exec) {
+      cudaGraphExecDestroy(exec);
+      exec = nullptr;
+    }
+    inner->prepare_graph(c);
+    c.capture_begin();
+    cudaGraph_t g = nullptr;
+    try {
+      inner->solve_graph(c, X, B, true);
+    } catch (...) {
+      while (!c.st_stack.empty()) {
+        cudaGraph_t b = nullptr;
+        cudaStreamEndCapture(c.st, &b);
+        c.st = c.st_stack.back();
+        c.st_stack.pop_back();
+      }
+      c.capturing = false;
+      cudaStreamEndCapture(c.st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    top_kernels = c.capture_end(&g);
+    const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    BSGPU_CUDA(e);
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    if (!zero || c.tracing || (Xs && (X != Xs || B != Bs))) {
+      inner->solve(c, X, B, zero);
+      this->this_level_iterations = inner->this_level_iterations;
+      this->converged = inner->converged;
+      return;
+    }
+    T* gx = Xs;
+    const T* gb = Bs;
+    if (!Xs) {
+      if (!xin.p) {
+        xin.alloc(std::max<int64_t>(N, 1));
+        bin.alloc(std::max<int64_t>(N, 1));
+      }
+      gx = xin.p;
+      gb = bin.p;
+      copy_vec(bin.p, B, N, c.st);
+      fill(T(0), xin.p, N, c.st);
+    }
+    const int k = key_src ? (*key_src ? 1 : 0) : 0;
+    if (!exec || k != key) {
+      capture(c, gx, const_cast<T*>(gb));
+      key = k;
+    }
+    BSGPU_CUDA(cudaGraphLaunch(exec, c.st));
+    add_launches(top_kernels);
+    c.graph_ran = true;
+    BSGPU_CUDA(cudaMemcpyAsync(c.h_err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    c.err_pending = true;
+    if (!Xs) copy_vec(X, (const T*)xin.p, N, c.st);
+    this->converged = true;
+    this->this_level_iterations = 1;
   }
 };
 
@@ -1572,6 +2035,8 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
   require(cfg.n_levels >= 1 && cfg.n_levels <= 8, "n_levels must be in 1..8");
   auto t = std::make_unique<Tree>();
   t->ctx = std::make_unique<Ctx>();
+  t->ctx->autotune = cfg.autotune != 0;
+  if (cfg.solver == BSGPU_SOLVER_FGMRES_PMG || cfg.solver == BSGPU_SOLVER_SOFTGMRES) t->ctx->tune(*A, 0);
   const char* tr = std::getenv("BSGPU_TRACE");
   t->ctx->tracing = tr != nullptr && tr[0] != '\0' && tr[0] != '0';
   t->A = A;
@@ -1627,10 +2092,30 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
       f->trace = t->ctx->trace_id("FlexGMRES");
       if (mixed) {
         auto ad = std::make_unique<MixedAdapter>(A->N);
-        ad->inner = build_level<float>(*t, A, level_matrix<float>(*t, A), 0, one);
+        auto lvl = build_level<float>(*t, A, level_matrix<float>(*t, A), 0, one);
+        if (cfg.graph) {
+          require(lvl->graphable(), "the V-cycle cannot be recorded as a graph with this coarse solver",
+                  BSGPU_ERR_UNSUPPORTED);
+          auto g = std::make_unique<GraphedT<float>>(A->N, std::move(lvl));
+          g->Xs = ad->x32.p;
+          g->Bs = ad->b32.p;
+          g->key_src = &t->learned_on;
+          ad->inner = std::move(g);
+        } else {
+          ad->inner = std::move(lvl);
+        }
         f->pc = std::move(ad);
       } else {
-        f->pc = build_level<double>(*t, A, A, 0, one);
+        auto lvl = build_level<double>(*t, A, A, 0, one);
+        if (cfg.graph) {
+          require(lvl->graphable(), "the V-cycle cannot be recorded as a graph with this coarse solver",
+                  BSGPU_ERR_UNSUPPORTED);
+          auto g = std::make_unique<GraphedT<double>>(A->N, std::move(lvl));
+          g->key_src = &t->learned_on;
+          f->pc = std::move(g);
+        } else {
+          f->pc = std::move(lvl);
+        }
       }
       f->tree = t.get();
       if (t->net && (cfg.learned & BSGPU_LEARNED_FGMRES)) {

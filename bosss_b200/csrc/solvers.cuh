@@ -9,6 +9,7 @@
 #include "amg.cuh"
 #include "blas1.cuh"
 #include "blockops.cuh"
+#include "devctl.cuh"
 #include "learned.cuh"
 #include "matrix.cuh"
 
@@ -24,6 +25,10 @@ struct Ctx {
   int nscal = 0, nflag = 0;
   int scal_cap = 4096;
   uint64_t seed = 12345;
+  bool autotune = false;  // tune the launch shapes of the level matrices' kernels at set-up
+  void tune(const Matrix& A, int mode, const void* dinv = nullptr) {
+    if (autotune) bsgpu::autotune(A, mode, dinv, st);
+  }
   Ctx();
   ~Ctx();
   double* scal(int n);  // allocate n device scalars
@@ -47,6 +52,35 @@ struct Ctx {
   bool tracing = false;
   std::vector<TraceEntry> trace;
   int trace_id(const std::string& name);
+
+  // Graph capture with device-side control flow (devctl.cuh).  While `capturing`, solvers record their kernels
+  // into the graph being captured on `st`; cond_begin adds a conditional node (IF or WHILE) after the work
+  // recorded so far and redirects `st` to a stream that captures the node's body until cond_end.  Kernels are
+  // counted per body at capture time; the device counts how often each body runs (cond_set), so the launch
+  // counter can add the kernels a replay actually ran (flush_graph_counts).
+  bool capturing = false;
+  std::vector<cudaStream_t> body_streams;
+  std::vector<cudaStream_t> st_stack;
+  std::vector<int> body_stack;
+  std::vector<long long> body_kernels;  // kernels recorded directly in each body (0: the top level)
+  int cur_body = 0;
+  unsigned long long mark = 0;
+  DBuf<unsigned int> d_exec;            // executions of each conditional body
+  std::vector<unsigned int> h_exec;
+  int* d_err = nullptr;                 // error word of captured solves (kDevErr* bits)
+  int* h_err = nullptr;                 // pinned mirror
+  bool err_pending = false;             // a copy of the error word is queued behind a graph launch
+  bool graph_ran = false;
+  void graph_init();
+  void capture_begin();
+  long long capture_end(cudaGraph_t* g);  // returns the kernels recorded at the top level
+  int new_body();
+  unsigned int* exec_of(int body) { return d_exec.p + body; }
+  cudaGraphConditionalHandle cond_handle();
+  void cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, int body);
+  void cond_end();
+  void check_graph_errors();  // after a synchronisation: raises the pending device error, if any
+  void flush_graph_counts();  // synchronises; adds the kernels of the conditional bodies that ran
 };
 
 // Scoped trace block; no-op unless ctx.tracing.
@@ -65,6 +99,12 @@ struct Solver {
   // X: initial guess in, solution out (device); B: right-hand side (device).  zero_guess: X is known to be 0.
   virtual void solve(Ctx& c, T* X, const T* B, bool zero_guess) = 0;
   virtual int nested() const { return 0; }
+  // Graph capture (Ctx::capturing): whether solve_graph can be recorded into a CUDA graph, the buffers it needs
+  // (allocated before the capture), and the recorded form of solve, whose decisions are taken on the device.
+  // Solvers without host decisions record solve itself.
+  virtual bool graphable() const { return false; }
+  virtual void prepare_graph(Ctx&) {}
+  virtual void solve_graph(Ctx& c, T* X, const T* B, bool zero) { solve(c, X, B, zero); }
   int this_level_iterations = 0;
   bool converged = false;
   std::vector<double> history;
@@ -78,6 +118,7 @@ struct Term {
   int max_iter = 300, min_iter = 1;
   double reduction = 0.1;
   std::pair<bool, bool> operator()(int iter, double R0, double R) const;
+  TermParams params() const { return TermParams{mode, max_iter, min_iter, tol, reduction}; }
 };
 
 // What the MultigridOperator holds beyond the transformed matrix: the untransformed finest matrix, its left

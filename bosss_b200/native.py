@@ -23,6 +23,7 @@ LEARNED_OFF, LEARNED_FGMRES, LEARNED_PRESMOOTH, LEARNED_BOTH = 0, 1, 2, 3
 # every symbol the header declares (checked by the CPU test-suite)
 EXPORTS = [
     "bsgpu_get_version", "bsgpu_last_error", "bsgpu_get_launch_count", "bsgpu_set_device",
+    "bsgpu_matrix_autotune", "bsgpu_autotune_report",
     "bsgpu_matrix_create", "bsgpu_matrix_destroy", "bsgpu_matrix_get_info", "bsgpu_matrix_read_values",
     "bsgpu_matrix_spmv", "bsgpu_matrix_spmv_noalloc", "bsgpu_matrix_spmv_device", "bsgpu_matrix_create_single",
     "bsgpu_matrix_spmv_device_f32",
@@ -47,7 +48,7 @@ class SolverConfig(C.Structure):
                 ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
                 ("learned", C.c_int32), ("learned_hidden", C.c_int32), ("learned_stall", C.c_double),
                 ("ortho_max_krylov", C.c_int32), ("recalc_resi_period", C.c_int32), ("learned_pairs", C.c_int32),
-                ("graph", C.c_int32), ("reserved", C.c_int32 * 2)]
+                ("graph", C.c_int32), ("autotune", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class SolveStats(C.Structure):
@@ -84,6 +85,8 @@ def lib() -> C.CDLL:
             "bsgpu_last_error": [C.c_char_p, C.c_size_t],
             "bsgpu_get_launch_count": [vp],
             "bsgpu_set_device": [C.c_int],
+            "bsgpu_matrix_autotune": [vp],
+            "bsgpu_autotune_report": [C.c_char_p, C.c_size_t],
             "bsgpu_matrix_create": [vp, i64, i32, vp, vp, vp, vp, i32],
             "bsgpu_matrix_destroy": [vp],
             "bsgpu_matrix_get_info": [vp, vp, vp, vp, vp],
@@ -151,3 +154,11 @@ def ptr(a) -> int:
     if hasattr(a, "data_ptr"):
         return a.data_ptr()
     return a.ctypes.data
+
+
+def autotune_report():
+    """Every launch-shape decision of the autotuner in this process (list of dicts)."""
+    import json
+    buf = C.create_string_buffer(1 << 20)
+    check(lib().bsgpu_autotune_report(buf, len(buf)))
+    return json.loads(buf.value.decode())

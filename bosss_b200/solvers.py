@@ -108,6 +108,10 @@ class BlockMsrMatrix:
         nat.check(nat.lib().bsgpu_matrix_create_single(self._h, C.byref(h)))
         return BlockMsrMatrix(h, single=True)
 
+    def Autotune(self):
+        """Picks the launch shape of this matrix's FP64 product by timing the candidates (autotune_report)."""
+        nat.check(nat.lib().bsgpu_matrix_autotune(self._h))
+
     def Restrict(self, keep: int) -> "BlockMsrMatrix":
         """Sub-matrix of the leading ``keep`` modes per species (GridAndDegRestriction's coarse operator)."""
         h = C.c_void_p()
@@ -318,6 +322,8 @@ class FGMRESConfig(IterativeSolverConfig):
     LearnedHidden: int = 64
     LearnedStall: float = 0.99
     LearnedPairs: int = 0           # training residuals collected in total (0: 12 per right-hand side)
+    Graph: bool = False             # record the V-cycle once as a CUDA graph with device-side decisions
+    Autotune: bool = False          # time the launch shapes of the level matrices' kernels at set-up
 
     def _config(self):
         if len(self.Preconditioners) != 1:
@@ -337,6 +343,8 @@ class FGMRESConfig(IterativeSolverConfig):
         if self.LearnedPairs < 0:
             raise ValueError("LearnedPairs must be >= 0")
         c.learned_pairs = self.LearnedPairs
+        c.graph = 1 if self.Graph else 0
+        c.autotune = 1 if self.Autotune else 0
         return c
 
 

@@ -60,6 +60,11 @@ BSGPU_API int bsgpu_last_error(char* buf, size_t len);
 BSGPU_API int bsgpu_get_launch_count(uint64_t* n);
 /* Selects the CUDA device used by handles created afterwards on this host thread. */
 BSGPU_API int bsgpu_set_device(int device);
+/* Launch-shape autotuner (no counterpart in the reference; BoSSS has no GPU kernels to tune): tunes the FP64
+ * product of A on the current device, and reports every decision taken in this process (solvers created with
+ * cfg.autotune = 1 tune their level matrices) as a JSON array of {matrix, times_ms per candidate, threads_per_cta}. */
+BSGPU_API int bsgpu_matrix_autotune(bsgpu_matrix_t A);
+BSGPU_API int bsgpu_autotune_report(char* buf, size_t len);
 
 /* ---- BlockMsrMatrix (BlockMsrMatrix.cs:191) ------------------------------------------------------------ *
  * nb block rows/columns; block i has nspc[i]*Np rows (nspc == NULL: one species); row_ptr[nb+1] and
@@ -185,8 +190,12 @@ typedef struct {
                                  recomputed from scratch every this many history entries, else updated (default 1) */
   int32_t learned_pairs;    /* training residuals bsgpu_solver_train_learned collects in total, spread over its
                                n_rhs solves (0: 12 per right-hand side)                           */
-  int32_t graph;            /* reserved (0)                                                     */
-  int32_t reserved[2];
+  int32_t graph;            /* 1: record the p-multigrid V-cycle of BSGPU_SOLVER_FGMRES_PMG once as a CUDA graph
+                               with its decisions (termination tests, re-orthonormalisation, residual checks) taken
+                               on the device, and replay it per application; 0: host-driven (default)       */
+  int32_t autotune;         /* 1: pick the launch shape (threads per CTA) of every level matrix's product and
+                               block-Jacobi kernels by timing the candidates at set-up (bsgpu_autotune_report) */
+  int32_t reserved[1];
 } bsgpu_solver_config;
 
 typedef struct {

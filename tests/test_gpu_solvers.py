@@ -51,7 +51,7 @@ def test_restriction_matches_oracle(cuda):
     assert np.array_equal(sub2.read_values(len(ref2)), ref2)
 
 
-@pytest.mark.parametrize("Np,spc", [(4, 1), (10, 1), (20, 1), (10, 2)])
+@pytest.mark.parametrize("Np,spc", [(4, 1), (10, 1), (20, 1), (10, 2), (1, 2), (4, 2), (20, 2)])
 def test_blockjacobi_matches_oracle(cuda, Np, spc):
     v = random_var_bsr(80, Np, seed=Np, max_spc=spc, spd=True)
     ref = O.blockjacobi(O.Bsr.of(v), np.zeros(v.N), v.rhs, iters=1)

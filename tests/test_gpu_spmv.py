@@ -107,3 +107,20 @@ def test_spmv_full_size_properties(cuda):
         err += np.sum((yh[i * 20:(i + 1) * 20] - acc) ** 2)
         nrm += np.sum(acc ** 2)
     assert np.sqrt(err / nrm) < TOL
+
+
+@pytest.mark.parametrize("Np", [1, 4, 10, 20])
+def test_spmv_two_species_blocks_all_typed_sizes(cuda, Np):
+    """Blocks of one or two species of Np modes (the XDG block types) for every Np the species-count kernels are
+    specialised on, FP64 against the oracle and FP32 against the FP64 product, with empty rows."""
+    import torch
+    v = random_var_bsr(240, Np, seed=20 + Np, max_spc=2, nnz_per_row=6, empty_rows=True)
+    M = _check(v, 0.9, -0.4, seed=Np)
+    rng = np.random.default_rng(Np)
+    x = rng.standard_normal(v.N)
+    ref = v.to_scipy() @ x
+    M32 = M.ToSingle()
+    xt = torch.from_numpy(x).float().cuda()
+    yt = torch.zeros_like(xt)
+    M32.SpMV(1.0, xt, 0.0, yt)
+    assert np.linalg.norm(yt.cpu().numpy() - ref) <= 1e-5 * np.linalg.norm(ref)
