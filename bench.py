@@ -58,6 +58,12 @@ def parse():
     ap.add_argument("--batch", type=int, default=256, help="xdgbatch: number of problems")
     ap.add_argument("--concurrency", type=int, default=16, help="xdgbatch: problems solved at once")
     ap.add_argument("--learned", default="off", help="varcoef96/xdgbatch: learned stage mode")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="fast form without the graph-recorded V-cycle")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="fast form without the launch-shape autotuner")
+    ap.add_argument("--no-learned-variant", dest="learned_variant", action="store_false",
+                    help="default workload: skip the learned-stage variant")
     return ap.parse_args()
 
 
@@ -304,16 +310,19 @@ def run_ours(args):
         return
 
     pmg = PmgConfig(DegreeHierarchy=levels_for(args.p), **SOLVER_PARAMS)
-    mk = lambda mixed: FGMRESConfig(ConvergenceCriterion=TOL, termination="relative", MaxKrylovDim=30,
-                                    Preconditioners=[pmg], MixedPrecision=mixed).CreateInstance(op)
-    t0 = time.perf_counter()
-    fast = mk(True)
-    torch.cuda.synchronize()
-    t_setup_fast = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    plain = mk(False)
-    torch.cuda.synchronize()
-    t_setup_plain = time.perf_counter() - t0
+
+    def mk(mixed, graph=False, tune=False, learned="off"):
+        return FGMRESConfig(ConvergenceCriterion=TOL, termination="relative", MaxKrylovDim=30, Preconditioners=[pmg],
+                            MixedPrecision=mixed, Graph=graph, Autotune=tune, Learned=learned,
+                            LearnedPairs=200).CreateInstance(op)
+
+    def timed_setup(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = fn()
+        torch.cuda.synchronize()
+        return out, time.perf_counter() - t0
+
     B = torch.from_numpy(s.rhs).to(dev)
     X = torch.zeros_like(B)
 
@@ -322,21 +331,50 @@ def run_ours(args):
         slv.Solve(X, B)
         return slv
 
-    # plain FP64 path: one warm-up, two timed
-    solve(plain)
-    plain_t = []
-    for _ in range(2):
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        solve(plain)
-        b.record(stream)
-        torch.cuda.synchronize()
-        plain_t.append(a.elapsed_time(b) * 1e-3)
+    def time_variant(slv, reps=2):
+        solve(slv)  # warm-up
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            solve(slv)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b) * 1e-3)
+        return min(ts)
+
+    # the plain FP64 GPU multigrid: the reference's algorithm in FP64, host-driven V-cycle
+    plain, t_setup_plain = timed_setup(lambda: mk(False))
+    plain_t = time_variant(plain)
     plain_iters = plain.ThisLevelIterations
     plain_res = _true_relres(Aop, op, X, B, s)
     x_plain = X.clone()
+    plain.Dispose()
 
+    # other forms, for the attribution of the speed-up (each: set-up, one warm-up, best of two)
+    variants = {}
+    forms = {"fp64_graph": dict(mixed=False, graph=True, tune=args.autotune),
+             "mixed_host": dict(mixed=True)}
+    for name, kw in forms.items():
+        slv, t_set = timed_setup(lambda: mk(**kw))
+        t = time_variant(slv)
+        variants[name] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
+                          "setup_s": t_set, "final_relres": _true_relres(Aop, op, X, B, s)}
+        slv.Dispose()
+    if args.learned_variant:
+        # the learned stage (FGMRES round-robin and pre-smoother) on top of the fast form, trained on 200
+        # residuals the solver generates
+        slv, t_set = timed_setup(lambda: mk(True, args.graph, args.autotune, learned="both"))
+        _, t_train = timed_setup(lambda: slv.TrainLearned(n_rhs=20, steps=400, lr=2e-3, seed=1))
+        t = time_variant(slv)
+        variants["learned_mixed"] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
+                                     "setup_s": t_set, "train_s": t_train, "pairs": slv.LearnedInfo()["pairs"],
+                                     "final_relres": _true_relres(Aop, op, X, B, s)}
+        slv.Dispose()
+
+    # the fast form: FP32 preconditioner, V-cycle recorded as one CUDA graph, autotuned launch shapes
+    fast, t_setup_fast = timed_setup(lambda: mk(True, args.graph, args.autotune))
     for _ in range(args.warmup):
         solve(fast)
     torch.cuda.synchronize()
@@ -374,7 +412,7 @@ def run_ours(args):
         if i > 0:
             e2e.append(a.elapsed_time(b) * 1e-3)
     e2e_t = max_over_ranks(sum(e2e) / len(e2e), ws)
-    plain_max = max_over_ranks(min(plain_t), ws)
+    plain_max = max_over_ranks(plain_t, ws)
 
     clocks = clk.summary()
     if rank != 0:
@@ -404,7 +442,9 @@ def run_ours(args):
         "config": default_config(s),
         "iters": fast_iters, "final_relres": fast_res,
         "plain_fp64": {"value": plain_max, "unit": "s", "iters": plain_iters,
-                       "final_relres": plain_res},
+                       "final_relres": plain_res, "form": "FP64 preconditioner, host-driven V-cycle"},
+        "fast_form": {"mixed": True, "graph": args.graph, "autotune": args.autotune},
+        "variants": variants,
         "speedup_vs_plain_fp64": plain_max / t_fast_max,
         "rel_diff_vs_plain_fp64_solution": sol_diff,
         "spmv": {"gbs": spmv_gbs, "ms": spmv_avg, "bytes": nbytes, "repeats": args.spmv_repeats,
@@ -419,6 +459,7 @@ def run_ours(args):
                      "peak_source": peaks[1]},
         "e2e": {"value": e2e_t, "unit": "s", "h2d_bytes_per_step": 2 * s.N * 8, "d2h_bytes_per_step": s.N * 8},
         "gpu_launches": launches,
+        "autotune": [{"matrix": r["matrix"], "threads_per_cta": r["threads_per_cta"]} for r in nat.autotune_report()],
         "clocks": clocks,
         "cpu_baseline": cpu_line,
     }
@@ -473,11 +514,11 @@ def spmv_bytes_blocks(s) -> int:
     return blk * 8 + len(s.col_idx) * 4 + (s.nb + 1) * 8 + 2 * int(lens.sum()) * 8
 
 
-def _fgmres(op, pmg: dict, mixed: bool, learned: str = "off"):
+def _fgmres(op, pmg: dict, mixed: bool, learned: str = "off", graph: bool = False, tune: bool = False):
     from bosss_b200.solvers import FGMRESConfig, PmgConfig
     return FGMRESConfig(ConvergenceCriterion=TOL, termination="relative", MaxKrylovDim=30, MaxSolverIterations=300,
                         Preconditioners=[PmgConfig(DegreeHierarchy=(10, 4, 1), **pmg)], MixedPrecision=mixed,
-                        Learned=learned).CreateInstance(op)
+                        Learned=learned, LearnedPairs=200, Graph=graph, Autotune=tune).CreateInstance(op)
 
 
 def _time_solve(slv, X, B, stream, reps=1):
@@ -532,19 +573,20 @@ def run_single_system(args, s, workload, prepare=None):
     B = torch.from_numpy(s.rhs).to(dev)
     X = torch.zeros_like(B)
     variants = {"plain_fp64": (PMG_BJ, False, "off"), "fp64_schwarz": (PMG_SCHWARZ, False, "off"),
-                "fast": (PMG_SCHWARZ, True, args.learned)}
+                "mixed_bj": (PMG_BJ, True, "off"), "fast": (PMG_SCHWARZ, True, args.learned)}
     res = {}
     x_plain = None
     fast = None
     train_s = None
     for name, (pmg, mixed, learned) in variants.items():
         t0 = time.perf_counter()
-        slv = _fgmres(op, pmg, mixed, learned)
+        fastform = name in ("fast", "mixed_bj")
+        slv = _fgmres(op, pmg, mixed, learned, graph=fastform and args.graph, tune=fastform and args.autotune)
         torch.cuda.synchronize()
         setup = time.perf_counter() - t0
         if learned != "off":
             t0 = time.perf_counter()
-            slv.TrainLearned(n_rhs=4, steps=200, lr=2e-3, seed=1)
+            slv.TrainLearned(n_rhs=20, steps=400, lr=2e-3, seed=1)
             torch.cuda.synchronize()
             train_s = time.perf_counter() - t0
         if name == "fast":
@@ -599,7 +641,9 @@ def run_single_system(args, s, workload, prepare=None):
         "config": {"workload": workload, "dof": s.N, "blocks": len(s.col_idx), "tol": TOL,
                    "l2": f"inputs larger than L2 ({nbytes / 1e9:.2f} GB per SpMV)", "parallelism": f"replicas x{ws}",
                    "fast": "FP32 Schwarz p-MG inside FP64 FlexGMRES" + ("" if args.learned == "off" else
-                                                                        f" + learned stage ({args.learned})"),
+                                                                        f" + learned stage ({args.learned})")
+                           + (", V-cycle as one CUDA graph" if args.graph else "")
+                           + (", autotuned launch shapes" if args.autotune else ""),
                    "plain": "FP64 block-Jacobi p-MG inside FP64 FlexGMRES"},
         "iters": fast.ThisLevelIterations, "final_relres": fast_res, "fast_setup_s": fast_setup,
         "learned_train_s": train_s,

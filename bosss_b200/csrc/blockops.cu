@@ -421,6 +421,150 @@ __global__ void ilu0_two_colour_kernel(const int64_t* __restrict__ rp, const int
   }
 }
 
+// Block ILU(0) in the natural block-row order (CellILU.ComputeILU, CellILU.cs:1229-1330), one wavefront of block
+// rows per launch: the rows of a wavefront have all their lower neighbours in earlier wavefronts, so each CTA
+// factors one row completely (row-wise "IKJ" order, which performs the same updates of every block in the same
+// order as the reference's column-wise loop):
+//   for every lower neighbour k of i, ascending:  L_ik = A_ik U_kk^{-1};  A_ij -= L_ik U_kj  (j > k, (k,j) in the
+//   pattern), and finally U_ii^{-1} for the rows after it.
+// M holds the factors in place (a copy of A's values beforehand); uinv receives U_ii^{-1} column-major at doff
+// (FP64, and FP32 when u32 != null).
+__global__ void ilu0_level_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                  const int32_t* __restrict__ len, const int64_t* __restrict__ boff, int V,
+                                  const int64_t* __restrict__ doff, const int32_t* __restrict__ rows, int64_t nrows,
+                                  double* __restrict__ M, double* __restrict__ uinv, float* __restrict__ u32,
+                                  int* __restrict__ err) {
+  extern __shared__ double sm[];
+  __shared__ int piv, bad;
+  for (int64_t q = blockIdx.x; q < nrows; q += gridDim.x) {
+    const int64_t i = rows[q];
+    const int I = len[i];
+    double* L = sm;  // I x K row-major (K <= max block length)
+    int64_t kd = -1;
+    for (int64_t t = rp[i]; t < rp[i + 1]; ++t)
+      if (ci[t] == i) kd = t;
+    if (threadIdx.x == 0) bad = (kd < 0);
+    __syncthreads();
+    if (bad) {
+      if (threadIdx.x == 0) atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff));
+      __syncthreads();
+      continue;
+    }
+    for (int64_t pk = rp[i]; pk < rp[i + 1]; ++pk) {
+      const int64_t k = ci[pk];
+      if (k >= i) break;  // block columns ascend: the lower neighbours come first
+      const int K = len[k];
+      const double* D = uinv + doff[k];
+      for (int e = threadIdx.x; e < I * K; e += blockDim.x) {
+        const int r = e / K, c = e - r * K;
+        double acc = 0.0;
+        for (int t = 0; t < K; ++t)
+          acc = fma(M[boff[pk] + (int64_t)(t / V) * I * V + r * V + (t % V)], D[(int64_t)c * K + t], acc);
+        L[e] = acc;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < I * K; e += blockDim.x) {
+        const int r = e / K, c = e - r * K;
+        M[boff[pk] + (int64_t)(c / V) * I * V + r * V + (c % V)] = L[e];
+      }
+      for (int64_t pj = pk + 1; pj < rp[i + 1]; ++pj) {
+        const int64_t j = ci[pj];
+        int64_t kj = -1;
+        {
+          int64_t lo = rp[k], hi = rp[k + 1];  // binary search of column j in row k
+          while (lo < hi) {
+            const int64_t mid = (lo + hi) / 2;
+            if (ci[mid] < j)
+              lo = mid + 1;
+            else
+              hi = mid;
+          }
+          if (lo < rp[k + 1] && ci[lo] == j) kj = lo;
+        }
+        if (kj < 0) continue;  // (k, j) outside the ILU(0) pattern
+        const int J = len[j];
+        for (int e = threadIdx.x; e < I * J; e += blockDim.x) {
+          const int r = e / J, c = e - r * J;
+          double acc = 0.0;
+          for (int t = 0; t < K; ++t) acc = fma(L[r * K + t], M[boff[kj] + (int64_t)(c / V) * K * V + t * V + (c % V)], acc);
+          M[boff[pj] + (int64_t)(c / V) * I * V + r * V + (c % V)] -= acc;
+        }
+      }
+      __syncthreads();
+    }
+    // U_ii^{-1}: Gauss-Jordan with partial pivoting in shared memory
+    double* U = sm;
+    double* prow = sm + I * I;
+    double* pcol = prow + I;
+    int* perm = reinterpret_cast<int*>(pcol + I);
+    for (int e = threadIdx.x; e < I * I; e += blockDim.x) {
+      const int r = e / I, c = e - r * I;
+      U[e] = M[boff[kd] + (int64_t)(c / V) * I * V + r * V + (c % V)];
+    }
+    __syncthreads();
+    for (int p = 0; p < I; ++p) {
+      if (threadIdx.x == 0) {
+        int best = p;
+        double mx = fabs(U[p * I + p]);
+        for (int r = p + 1; r < I; ++r)
+          if (fabs(U[r * I + p]) > mx) {
+            mx = fabs(U[r * I + p]);
+            best = r;
+          }
+        piv = best;
+        perm[p] = best;
+        if (!(mx > 0.0) || !isfinite(mx)) {
+          bad = 1;
+          atomicCAS(err, 0, (int)(i + 1 < 0x7fffffff ? i + 1 : 0x7fffffff));
+        }
+      }
+      __syncthreads();
+      if (bad) break;
+      if (piv != p)
+        for (int c = threadIdx.x; c < I; c += blockDim.x) {
+          const double t = U[p * I + c];
+          U[p * I + c] = U[piv * I + c];
+          U[piv * I + c] = t;
+        }
+      __syncthreads();
+      const double inv = 1.0 / U[p * I + p];
+      for (int t = threadIdx.x; t < I; t += blockDim.x) {
+        prow[t] = (t == p) ? inv : U[p * I + t] * inv;
+        pcol[t] = U[t * I + p];
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < I * I; e += blockDim.x) {
+        const int r = e / I, c = e - r * I;
+        if (r == p)
+          U[e] = prow[c];
+        else if (c == p)
+          U[e] = -pcol[r] * prow[p];
+        else
+          U[e] -= pcol[r] * prow[c];
+      }
+      __syncthreads();
+    }
+    if (!bad) {
+      for (int p = I - 1; p >= 0; --p) {
+        const int t = perm[p];
+        if (t != p)
+          for (int r = threadIdx.x; r < I; r += blockDim.x) {
+            const double w = U[r * I + p];
+            U[r * I + p] = U[r * I + t];
+            U[r * I + t] = w;
+          }
+        __syncthreads();
+      }
+      for (int e = threadIdx.x; e < I * I; e += blockDim.x) {
+        const int r = e / I, c = e - r * I;
+        uinv[doff[i] + (int64_t)c * I + r] = U[e];
+        if (u32) u32[doff[i] + (int64_t)c * I + r] = (float)U[e];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 DBuf<int32_t> blk_rows(const Matrix& A) {
   std::vector<int32_t> br(A.nnzb);
   for (int64_t i = 0; i < A.nb; ++i)
@@ -470,6 +614,24 @@ void invert_diag_blocks(const Matrix& A, double* D64, float* D32, int* err, cuda
   invert_kernel<<<grid_for(A.nb), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.v64.p, A.V, A.doff.p, D64, D32,
                                                   err, A.nb);
   BSGPU_CHECK_LAUNCH();
+}
+
+void ilu0_levels(const Matrix& A, const int32_t* rows, const std::vector<int64_t>& level_ptr, Matrix& M,
+                 double* uinv, float* u32, int* err, cudaStream_t st) {
+  require(!A.single && !M.single && M.V == A.V && M.nvals == A.nvals, "ILU(0) factors need FP64 matrices");
+  BSGPU_CUDA(cudaMemcpyAsync(M.v64.p, A.v64.p, (size_t)A.nvals * 8, cudaMemcpyDeviceToDevice, st));
+  const int64_t n = A.max_len();
+  const size_t smem = (size_t)(n * n + 2 * n) * sizeof(double) + (size_t)n * sizeof(int);
+  require(smem <= 200 * 1024, "block too large for ILU(0)", BSGPU_ERR_UNSUPPORTED);
+  if (smem > 48 * 1024)
+    BSGPU_CUDA(cudaFuncSetAttribute(ilu0_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (size_t l = 0; l + 1 < level_ptr.size(); ++l) {
+    const int64_t nr = level_ptr[l + 1] - level_ptr[l];
+    if (nr == 0) continue;
+    ilu0_level_kernel<<<grid_for(nr), 128, smem, st>>>(A.rp.p, A.ci.p, A.len.p, A.boff.p, A.V, A.doff.p,
+                                                       rows + level_ptr[l], nr, M.v64.p, uinv, u32, err);
+    BSGPU_CHECK_LAUNCH();
+  }
 }
 
 void ilu0_two_colour(const Matrix& A, const double* dinv, const int32_t* rows1, int64_t n1, Matrix& M, int* err,

@@ -22,6 +22,12 @@ void schwarz_factor(const Matrix& A, Matrix& M, int* err, cudaStream_t st);
 // colour-1 rows `rows1`.  dinv: inverses of A's diagonal blocks (invert_diag_blocks layout).
 void ilu0_two_colour(const Matrix& A, const double* dinv, const int32_t* rows1, int64_t n1, Matrix& M, int* err,
                      cudaStream_t st);
+// Block ILU(0) in the natural block-row order (CellILU.cs:1229-1330), wavefront by wavefront: rows[level_ptr[l] ..
+// level_ptr[l+1]) are the block rows whose lower neighbours all lie in earlier wavefronts.  M (FP64, A's
+// structure) <- the factors (unit-lower L below the diagonal, U on and above it); uinv (and u32 if not null) <-
+// U_ii^{-1} per block row, column-major at diag_offsets(A).
+void ilu0_levels(const Matrix& A, const int32_t* rows, const std::vector<int64_t>& level_ptr, Matrix& M,
+                 double* uinv, float* u32, int* err, cudaStream_t st);
 // y_i = L_i^{-T} x_i per block (initial-guess transform with a lower-triangular L, row-major).
 void block_trsv_lt(const Matrix& A, const double* L, const double* x, double* y, cudaStream_t st);
 

@@ -95,6 +95,7 @@ void solve_device(bsgpu_solver_s* s, double* dX, const double* dB, bsgpu_solve_s
   BSGPU_CUDA(cudaEventRecord(s->e1, c.st));
   BSGPU_CUDA(cudaEventSynchronize(s->e1));
   c.flush_graph_counts();
+  if (t.net) learned_check(*t.net, c.st);
   float ms = 0;
   BSGPU_CUDA(cudaEventElapsedTime(&ms, s->e0, s->e1));
   s->history = t.top->history;
@@ -442,6 +443,7 @@ BSGPU_API int bsgpu_solver_set_tracing(bsgpu_solver_t s, int32_t on) {
   return guarded([&] {
     require(s != nullptr, "null solver");
     s->tree->ctx->tracing = on != 0;
+    s->tree->ctx->graph_counts.clear();
     for (auto& e : s->tree->ctx->trace) {
       e.calls = 0;
       e.seconds = 0;
@@ -459,6 +461,13 @@ BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len) {
     for (auto& e : s->tree->ctx->trace) {
       std::snprintf(tmp, sizeof(tmp), "%s{\"name\": \"%s\", \"calls\": %ld, \"seconds\": %.6f, \"iterations\": %ld}",
                     first ? "" : ", ", e.name.c_str(), e.calls, e.seconds, e.iterations);
+      out += tmp;
+      first = false;
+    }
+    // executions of the conditional bodies of the recorded V-cycle (graph mode)
+    for (auto& g : s->tree->ctx->graph_counts) {
+      std::snprintf(tmp, sizeof(tmp), "%s{\"name\": \"graph: %s\", \"calls\": %llu, \"seconds\": 0, \"iterations\": 0}",
+                    first ? "" : ", ", g.first.c_str(), g.second);
       out += tmp;
       first = false;
     }
@@ -516,6 +525,7 @@ BSGPU_API int bsgpu_solver_learned_apply(bsgpu_solver_t s, const double* r, doub
     learned_apply(n, s->B.p, s->X.p, d + 1, c.st);
     BSGPU_CUDA(cudaMemcpyAsync(z, s->X.p, N * 8, cudaMemcpyDeviceToHost, c.st));
     BSGPU_CUDA(cudaStreamSynchronize(c.st));
+    learned_check(n, c.st);
   });
 }
 

@@ -6,12 +6,11 @@
 //     z_c = W3^T relu(W2^T relu(W1^T f_c)),   f_c = [r_c, r_n1, ..., r_n6, extra_c]
 // No biases: with ReLU the map is positively homogeneous, z(a r) = a z(r) for a > 0, so it commutes with the
 // arbitrary scaling of Krylov vectors.  Weights are BF16 (FP32 master copies for training), products accumulate in
-// FP32 on the tensor cores (wmma bf16 16x16x16 tiles), one CTA per tile of 64 cells with all weights in shared
-// memory.  Training minimises the energy norm of the error left after the correction,
+// FP32 on the 5th-generation tensor cores (tcgen05.mma with tensor-memory accumulators), one CTA per tile of 128
+// cells with all weights in shared memory.  Training minimises the energy norm of the error left after the correction,
 //     |e - z|_A^2 = z^T A z - 2 z^T r + e^T A e,   A e = r,
 // i.e. it fits a local approximate inverse of the operator, with one SpMV per step for A z.
 #include <cuda_bf16.h>
-#include <mma.h>
 
 #include <algorithm>
 #include <cmath>
@@ -24,11 +23,7 @@ namespace bsgpu {
 
 namespace {
 
-using namespace nvcuda;
-constexpr int kTile = 64;    // cells per CTA tile (forward)
 constexpr int kBTile = 32;   // cells per CTA tile (backward)
-
-__device__ __forceinline__ __nv_bfloat16 bf(float x) { return __float2bfloat16(x); }
 
 template <typename TV>
 __device__ __forceinline__ float feature(const TV* __restrict__ r, const int32_t* __restrict__ nbr,
@@ -61,78 +56,240 @@ struct FwdArgs {
   int Np, nfaces, nextra, F, Fp, H, Op;
 };
 
-// C[64 x N] = A[64 x K] * B[K x N], all in shared memory (A, B bf16 row-major, C float row-major); 8 warps
-template <int NW>
-__device__ __forceinline__ void tile_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
-                                          float* C, int ldc, int K, int N) {
-  const int warp = threadIdx.x >> 5;
-  const int mt = kTile / 16, nt = N / 16;
-  for (int t = warp; t < mt * nt; t += NW) {
-    const int i = t / nt, j = t % nt;
-    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc;
-    wmma::fill_fragment(acc, 0.0f);
-    for (int k = 0; k < K; k += 16) {
-      wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, wmma::row_major> a;
-      wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, wmma::row_major> b;
-      wmma::load_matrix_sync(a, A + (size_t)i * 16 * lda + k, lda);
-      wmma::load_matrix_sync(b, B + (size_t)k * ldb + j * 16, ldb);
-      wmma::mma_sync(acc, a, b, acc);
-    }
-    wmma::store_matrix_sync(C + (size_t)i * 16 * ldc + j * 16, acc, ldc, wmma::mem_row_major);
-  }
+// ---- tcgen05 forward pass -------------------------------------------------------------------------------------
+// One CTA of 128 threads per tile of 128 cells, thread t owning cell row t.  Each layer is one M = 128 block of
+// tcgen05.mma (kind::f16: BF16 operands, FP32 accumulation in tensor memory), K in steps of 16, issued by one
+// thread; the operands sit in shared memory in the canonical K-major layout without swizzle (8-row x 16-byte core
+// matrices, K-adjacent core matrices 128 bytes apart, 8-row groups K/8 x 128 bytes apart).  The accumulators are
+// read back with tcgen05.ld (32x32b: warp w sees tensor-memory lanes 32w .. 32w+31, i.e. its own cells), passed
+// through ReLU, rounded to BF16 and written as the next layer's A operand.  Tensor memory: layer 1 at columns
+// [0, H), layer 2 at [H, 2H), the output layer at [0, Op).
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of element (r, k) of an R x K BF16 operand in the canonical K-major layout
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int K) {
+  return (uint32_t)(((r >> 3) * (K >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
 }
 
+// shared-memory matrix descriptor: start address, leading (K) and stride (M/N) byte offsets, descriptor version 1,
+// no swizzle
+__device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), BF16 A and B (bits 7-9, 10-12 = 1), both
+// K-major (bits 15, 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+__device__ __forceinline__ void commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// bounded wait on an mbarrier phase
+__device__ __forceinline__ bool wait_phase(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < (1ll << 26); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 16 FP32 columns of this thread's tensor-memory lane
+__device__ __forceinline__ void ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// 8 consecutive K entries of one row as one 16-byte store
+__device__ __forceinline__ void st8(unsigned char* base, uint32_t off, const float* v) {
+  __nv_bfloat162 h[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) h[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+  *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(h);
+}
+
+constexpr int kRows = 128;  // cells per tile = MMA M = threads per CTA
+
+}  // namespace tc
+
+// shared memory of the tcgen05 forward kernel: W1^T [H x Fp], W2^T [H x H], W3^T [Op x H], A1 [128 x Fp],
+// A2 [128 x H] (BF16, canonical layout), each at a 1024-byte boundary
+struct TcSmem {
+  uint32_t w1, w2, w3, a1, a2, total;
+  __host__ __device__ TcSmem(int Fp, int H, int Op) {
+    auto up = [](uint32_t x) { return (x + 1023u) & ~1023u; };
+    w1 = 0;
+    w2 = up(w1 + (uint32_t)(H * Fp * 2));
+    w3 = up(w2 + (uint32_t)(H * H * 2));
+    a1 = up(w3 + (uint32_t)(Op * H * 2));
+    a2 = up(a1 + (uint32_t)(tc::kRows * Fp * 2));
+    total = up(a2 + (uint32_t)(tc::kRows * H * 2));
+  }
+};
+
 template <typename TV>
-__global__ void __launch_bounds__(256) mlp_fwd_kernel(FwdArgs a, const TV* __restrict__ r, TV* __restrict__ z) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  __nv_bfloat16* W1 = reinterpret_cast<__nv_bfloat16*>(smem);
-  __nv_bfloat16* W2 = W1 + a.Fp * a.H;
-  __nv_bfloat16* W3 = W2 + a.H * a.H;
-  __nv_bfloat16* X = W3 + a.H * a.Op;
-  __nv_bfloat16* Hb = X + kTile * a.Fp;
-  float* Cf = reinterpret_cast<float*>(Hb + kTile * a.H);
-  const int nthr = blockDim.x;
-  for (int e = threadIdx.x; e < a.Fp * a.H; e += nthr) W1[e] = a.w1[e];
-  for (int e = threadIdx.x; e < a.H * a.H; e += nthr) W2[e] = a.w2[e];
-  for (int e = threadIdx.x; e < a.H * a.Op; e += nthr) W3[e] = a.w3[e];
+__global__ void __launch_bounds__(128) mlp_fwd_tc_kernel(FwdArgs a, const TV* __restrict__ r, TV* __restrict__ z,
+                                                         int tmem_cols, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, warp = t >> 5;
+  const int Fp = a.Fp, H = a.H, Op = a.Op;
+  const TcSmem L(Fp, H, Op);
+  unsigned char* W1 = smem + L.w1;
+  unsigned char* W2 = smem + L.w2;
+  unsigned char* W3 = smem + L.w3;
+  unsigned char* A1 = smem + L.a1;
+  unsigned char* A2 = smem + L.a2;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_slot)),
+                 "r"(tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(&mbar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // weights as the B operands: B = W^T (N rows x K), element (n, k) = W[k][n]
+  const uint16_t* w1 = reinterpret_cast<const uint16_t*>(a.w1);
+  const uint16_t* w2 = reinterpret_cast<const uint16_t*>(a.w2);
+  const uint16_t* w3 = reinterpret_cast<const uint16_t*>(a.w3);
+  for (int e = t; e < Fp * H; e += blockDim.x) {
+    const int k = e / H, n = e - k * H;
+    *reinterpret_cast<uint16_t*>(W1 + tc::kmajor_off(n, k, Fp)) = w1[e];
+  }
+  for (int e = t; e < H * H; e += blockDim.x) {
+    const int k = e / H, n = e - k * H;
+    *reinterpret_cast<uint16_t*>(W2 + tc::kmajor_off(n, k, H)) = w2[e];
+  }
+  for (int e = t; e < H * Op; e += blockDim.x) {
+    const int k = e / Op, n = e - k * Op;
+    *reinterpret_cast<uint16_t*>(W3 + tc::kmajor_off(n, k, H)) = w3[e];
+  }
+  tc::fence_proxy();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t mb = tc::smem_u32(&mbar);
+  const uint32_t sA1 = tc::smem_u32(A1), sA2 = tc::smem_u32(A2);
+  const uint32_t sW1 = tc::smem_u32(W1), sW2 = tc::smem_u32(W2), sW3 = tc::smem_u32(W3);
   const double sc = a.scale ? *a.scale : 1.0;
   const float inv = sc > 0 ? (float)(1.0 / sc) : 1.0f;
-  const int ldc = a.H > a.Op ? a.H : a.Op;
-  for (int64_t t0 = (int64_t)blockIdx.x * kTile; t0 < a.ncells; t0 += (int64_t)gridDim.x * kTile) {
+  uint32_t parity = 0;
+  bool bad = false;  // a wait gave up (uniform across the CTA)
+  // one layer: D[128 x N] (tensor memory column dcol) = A[128 x K] * B^T, then wait for it
+  auto layer = [&](uint32_t sA, uint32_t sB, int K, int N, uint32_t dcol) -> bool {
+    tc::fence_proxy();
+    tc::fence_before();
     __syncthreads();
-    for (int e = threadIdx.x; e < kTile * a.Fp; e += nthr) {
-      const int cl = e / a.Fp, f = e - cl * a.Fp;
-      const int64_t c = t0 + cl;
-      float v = 0.0f;
-      if (c < a.ncells && f < a.F) v = feature<TV>(r, a.nbr, a.extra, c, f, a.Np, a.nfaces, a.nextra, inv);
-      X[e] = bf(v);
+    if (t == 0) {
+      tc::fence_after();
+      const uint32_t sbo = (uint32_t)(K / 8) * 128u;
+      for (int s = 0; s < K / 16; ++s)
+        tc::mma(tmem + dcol, tc::desc(sA + (uint32_t)s * 256u, 128u, sbo), tc::desc(sB + (uint32_t)s * 256u, 128u, sbo),
+                tc::idesc_bf16(tc::kRows, N), s > 0 ? 1u : 0u);
+      tc::commit(mb);
     }
-    __syncthreads();
-    tile_gemm<8>(X, a.Fp, W1, a.H, Cf, ldc, a.Fp, a.H);
-    __syncthreads();
-    for (int e = threadIdx.x; e < kTile * a.H; e += nthr) {
-      const int cl = e / a.H, j = e - cl * a.H;
-      const float h = fmaxf(Cf[cl * ldc + j], 0.0f);
-      Hb[e] = bf(h);
-      if (a.act && t0 + cl < a.ncells) a.act[(t0 + cl) * 2 * a.H + j] = h;
+    const bool ok = tc::wait_phase(mb, parity);
+    tc::fence_after();
+    if (__syncthreads_and(ok ? 1 : 0) == 0) return false;
+    parity ^= 1u;
+    return true;
+  };
+  for (int64_t t0 = (int64_t)blockIdx.x * tc::kRows; t0 < a.ncells; t0 += (int64_t)gridDim.x * tc::kRows) {
+    const int64_t c = t0 + t;
+    const bool valid = c < a.ncells;
+    // layer-1 operand: this cell's features, 8 at a time
+    for (int k0 = 0; k0 < Fp; k0 += 8) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int f = k0 + q;
+        v[q] = (valid && f < a.F) ? feature<TV>(r, a.nbr, a.extra, c, f, a.Np, a.nfaces, a.nextra, inv) : 0.0f;
+      }
+      tc::st8(A1, tc::kmajor_off(t, k0, Fp), v);
     }
-    __syncthreads();
-    tile_gemm<8>(Hb, a.H, W2, a.H, Cf, ldc, a.H, a.H);
-    __syncthreads();
-    for (int e = threadIdx.x; e < kTile * a.H; e += nthr) {
-      const int cl = e / a.H, j = e - cl * a.H;
-      const float h = fmaxf(Cf[cl * ldc + j], 0.0f);
-      Hb[e] = bf(h);
-      if (a.act && t0 + cl < a.ncells) a.act[(t0 + cl) * 2 * a.H + a.H + j] = h;
+    if (!layer(sA1, sW1, Fp, H, 0)) {
+      bad = true;
+      break;
     }
-    __syncthreads();
-    tile_gemm<8>(Hb, a.H, W3, a.Op, Cf, ldc, a.H, a.Op);
-    __syncthreads();
-    for (int e = threadIdx.x; e < kTile * a.Np; e += nthr) {
-      const int cl = e / a.Np, o = e - cl * a.Np;
-      const int64_t c = t0 + cl;
-      if (c < a.ncells) z[c * a.Np + o] = (TV)((double)Cf[cl * ldc + o] * sc);
+    for (int cb = 0; cb < H; cb += 16) {
+      float v[16];
+      tc::ld16(tmem + lane_base + (uint32_t)cb, v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = fmaxf(v[q], 0.0f);
+      if (a.act && valid)
+        for (int q = 0; q < 16; ++q) a.act[c * 2 * H + cb + q] = v[q];
+      tc::st8(A2, tc::kmajor_off(t, cb, H), v);
+      tc::st8(A2, tc::kmajor_off(t, cb + 8, H), v + 8);
     }
+    if (!layer(sA2, sW2, H, H, (uint32_t)H)) {
+      bad = true;
+      break;
+    }
+    for (int cb = 0; cb < H; cb += 16) {
+      float v[16];
+      tc::ld16(tmem + lane_base + (uint32_t)(H + cb), v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) v[q] = fmaxf(v[q], 0.0f);
+      if (a.act && valid)
+        for (int q = 0; q < 16; ++q) a.act[c * 2 * H + H + cb + q] = v[q];
+      tc::st8(A2, tc::kmajor_off(t, cb, H), v);
+      tc::st8(A2, tc::kmajor_off(t, cb + 8, H), v + 8);
+    }
+    if (!layer(sA2, sW3, H, Op, 0)) {
+      bad = true;
+      break;
+    }
+    float y[16];
+    tc::ld16(tmem + lane_base, y);
+    if (valid)
+      for (int o = 0; o < a.Np; ++o) z[c * a.Np + o] = (TV)((double)y[o] * sc);
+    tc::fence_before();
+    __syncthreads();
+  }
+  if (bad) {
+    // a wait gave up: flag it, and give the committed MMAs a bounded second chance to finish before the tensor
+    // memory is freed
+    if (t == 0) atomicExch(err, 1);
+    tc::wait_phase(mb, parity);
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols) : "memory");
   }
 }
 
@@ -269,9 +426,10 @@ uint16_t to_bf16_bits(float x) {
   return (uint16_t)((u + rounding) >> 16);
 }
 
-size_t fwd_smem(const LearnedNet& n) {
-  const int ldc = std::max(n.H, n.Op);
-  return (size_t)(n.Fp * n.H + n.H * n.H + n.H * n.Op + kTile * n.Fp + kTile * n.H) * 2 + (size_t)kTile * ldc * 4;
+int tmem_columns(int H) {
+  int c = 32;
+  while (c < 2 * H) c *= 2;
+  return c;
 }
 
 template <typename TV>
@@ -280,11 +438,11 @@ void apply_impl(const LearnedNet& net, const TV* r, TV* z, const double* scale, 
   FwdArgs a{net.nbr.p, net.extra.p, reinterpret_cast<const __nv_bfloat16*>(net.w1.p),
             reinterpret_cast<const __nv_bfloat16*>(net.w2.p), reinterpret_cast<const __nv_bfloat16*>(net.w3.p), act,
             scale, net.ncells, net.Np, net.nfaces, net.nextra, net.F, net.Fp, net.H, net.Op};
-  const size_t sm = fwd_smem(net);
-  BSGPU_CUDA(cudaFuncSetAttribute(mlp_fwd_kernel<TV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  const int64_t tiles = (net.ncells + kTile - 1) / kTile;
+  const TcSmem L(net.Fp, net.H, net.Op);
+  BSGPU_CUDA(cudaFuncSetAttribute(mlp_fwd_tc_kernel<TV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  const int64_t tiles = (net.ncells + tc::kRows - 1) / tc::kRows;
   const int grid = (int)std::min<int64_t>(tiles, (int64_t)num_sms() * 2);
-  mlp_fwd_kernel<TV><<<grid, 256, sm, st>>>(a, r, z);
+  mlp_fwd_tc_kernel<TV><<<grid, tc::kRows, L.total, st>>>(a, r, z, tmem_columns(net.H), net.err.p);
   BSGPU_CHECK_LAUNCH();
 }
 
@@ -299,7 +457,12 @@ void LearnedNet::init(int Np_, int64_t ncells_, int nfaces_, int nextra_, const 
   F = (nfaces + 1) * Np + nextra;
   Fp = (F + 15) / 16 * 16;
   Op = (Np + 15) / 16 * 16;
-  require(fwd_smem(*this) <= 200 * 1024, "learned stage: input too wide for one CTA", BSGPU_ERR_UNSUPPORTED);
+  require(H % 16 == 0 && H >= 16 && H <= 128, "learned stage: hidden width must be a multiple of 16 in 16..128",
+          BSGPU_ERR_UNSUPPORTED);
+  require(Op == 16, "learned stage: at most 16 modes per cell", BSGPU_ERR_UNSUPPORTED);
+  require(TcSmem(Fp, H, Op).total <= 200 * 1024, "learned stage: input too wide for one CTA", BSGPU_ERR_UNSUPPORTED);
+  err.alloc(1);
+  BSGPU_CUDA(cudaMemset(err.p, 0, sizeof(int)));
   nbr.alloc(std::max<int64_t>(ncells * nfaces, 1));
   BSGPU_CUDA(cudaMemcpy(nbr.p, nbr_host, ncells * nfaces * 4, cudaMemcpyHostToDevice));
   extra.alloc(std::max<int64_t>(ncells * nextra, 1));
@@ -336,6 +499,16 @@ void LearnedNet::init(int Np_, int64_t ncells_, int nfaces_, int nextra_, const 
   upload(h3, m3, w3, g3, a3, v3);
   adam_t = 0;
   trained = false;
+}
+
+void learned_check(const LearnedNet& net, cudaStream_t st) {
+  int h = 0;
+  BSGPU_CUDA(cudaMemcpyAsync(&h, net.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  if (h) {
+    BSGPU_CUDA(cudaMemset(net.err.p, 0, sizeof(int)));
+    throw Error(BSGPU_ERR_TIMEOUT, "learned stage: a tensor-core wait gave up");
+  }
 }
 
 void learned_scale(const double* nrm, double* scale, int64_t n, cudaStream_t st) {

@@ -19,6 +19,7 @@ struct LearnedNet {
   DBuf<uint16_t> w1, w2, w3;                 // [Fp x H], [H x H], [H x Op], row-major (k, n)
   DBuf<float> m1, m2, m3, g1, g2, g3, a1, a2, a3, v1, v2, v3;
   DBuf<float> act;                           // training activations [ncells x 2H]
+  DBuf<int> err;                             // set when a bounded wait of the forward kernel gave up
   int adam_t = 0;
   bool trained = false;
   void init(int Np_, int64_t ncells_, int nfaces_, int nextra_, const int32_t* nbr_host, const float* extra_host,
@@ -31,6 +32,8 @@ struct LearnedNet {
 void learned_apply(const LearnedNet& net, const double* r, double* z, const double* scale, cudaStream_t st);
 void learned_apply(const LearnedNet& net, const float* r, float* z, const double* scale, cudaStream_t st);
 
+// Raises BSGPU_ERR_TIMEOUT (and clears the flag) when a forward launch reported a wait that gave up.
+void learned_check(const LearnedNet& net, cudaStream_t st);
 // scale = |r| / sqrt(n) from a device norm (input normalisation of the stage)
 void learned_scale(const double* nrm, double* scale, int64_t n, cudaStream_t st);
 

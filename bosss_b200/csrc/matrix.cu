@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
   // no block row of the list reads another row of the list.
   int64_t i = (int64_t)blockIdx.x * BPC + lb;
   bool valid = (lb < BPC) && (i < nb);
-  if constexpr (MODE == 2) {
+  if constexpr (MODE == 2 || MODE == 3) {
     if (valid) i = row_list[i];
   }
   const uint64_t pol = policy_evict_first();
@@ -145,6 +145,12 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
       if (z != nullptr) out = fma(beta, z[g], out);
       y[g] = out;
     }
+  } else if constexpr (MODE == 3) {
+    // unit-diagonal in-place update over a row list (forward substitution with a unit lower factor): every read of
+    // x in the CTA precedes the barrier, the writes follow it
+    const T val = valid ? fma(alpha, z[g] - acc, x[g]) : T(0);
+    __syncthreads();
+    if (valid) y[g] = val;
   } else {
     __shared__ T q[256];
     q[t] = valid ? (z[g] - acc) : T(0);
@@ -741,6 +747,38 @@ void gs_update_rows(const Matrix& A, const double* dinv, double omega, const int
                     const double* b, double* x, cudaStream_t st) {
   require(!A.single, "precision mismatch");
   gs_rows_impl<double>(A, A.v64.p, dinv, omega, rows, nrows, b, x, st);
+}
+
+namespace {
+template <typename T>
+void unit_rows_impl(const Matrix& A, const T* vals, const int32_t* rows, int64_t nrows, const T* b, T* x,
+                    cudaStream_t st) {
+  require(specialised(A), "unit-diagonal row update needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
+  if (nrows == 0) return;
+  constexpr int VW = sizeof(T) == 8 ? 2 : 4;
+#define BSGPU_UNIT(NP, VV)                                                                                   \
+  spmv_uniform_kernel<T, NP, VV, 3><<<(unsigned)((nrows + 256 / NP - 1) / (256 / NP)), (256 / NP) * NP, 0, st>>>( \
+      A.rp.p, A.ci.p, vals, x, b, x, T(1), T(0), nrows, nullptr, nullptr, rows)
+  switch (A.Np) {
+    case 20: BSGPU_UNIT(20, VW); break;
+    case 4: BSGPU_UNIT(4, VW); break;
+    case 10: BSGPU_UNIT(10, 2); break;
+    case 6: BSGPU_UNIT(6, 2); break;
+  }
+#undef BSGPU_UNIT
+  BSGPU_CHECK_LAUNCH();
+}
+}  // namespace
+
+void unit_update_rows(const Matrix& A, const int32_t* rows, int64_t nrows, const double* b, double* x,
+                      cudaStream_t st) {
+  require(!A.single, "precision mismatch");
+  unit_rows_impl<double>(A, A.v64.p, rows, nrows, b, x, st);
+}
+void unit_update_rows(const Matrix& A, const int32_t* rows, int64_t nrows, const float* b, float* x,
+                      cudaStream_t st) {
+  require(A.single, "precision mismatch");
+  unit_rows_impl<float>(A, A.v32.p, rows, nrows, b, x, st);
 }
 void gs_update_rows(const Matrix& A, const float* dinv, float omega, const int32_t* rows, int64_t nrows,
                     const float* b, float* x, cudaStream_t st) {

@@ -73,6 +73,11 @@ void gs_update_rows(const Matrix& A, const double* dinv, double omega, const int
                     const double* b, double* x, cudaStream_t st);
 void gs_update_rows(const Matrix& A, const float* dinv, float omega, const int32_t* rows, int64_t nrows,
                     const float* b, float* x, cudaStream_t st);
+// In-place unit-diagonal update over listed block rows: x_i += (b - A*x)_i (no two listed rows neighbours).  With
+// x zero on the rows not yet visited this is the forward substitution of a unit lower factor stored in A.
+void unit_update_rows(const Matrix& A, const int32_t* rows, int64_t nrows, const double* b, double* x,
+                      cudaStream_t st);
+void unit_update_rows(const Matrix& A, const int32_t* rows, int64_t nrows, const float* b, float* x, cudaStream_t st);
 // Greedy colouring of the block graph (lists of block rows per colour).
 std::vector<std::vector<int32_t>> greedy_colouring(const Matrix& A);
 // y = omega * Dinv * b (first block-Jacobi sweep from a zero guess).

@@ -52,6 +52,7 @@ void Ctx::capture_begin() {
   graph_init();
   BSGPU_CUDA(cudaStreamSynchronize(st));
   body_kernels.assign(1, 0);
+  body_names.assign(1, "top");
   body_stack.clear();
   st_stack.clear();
   cur_body = 0;
@@ -71,11 +72,12 @@ long long Ctx::capture_end(cudaGraph_t* g) {
   return body_kernels[0];
 }
 
-int Ctx::new_body() {
+int Ctx::new_body(const std::string& name) {
   require(capturing, "conditional body outside a graph capture");
   require((int)body_kernels.size() < kMaxBodies, "graph capture: too many conditional bodies",
           BSGPU_ERR_UNSUPPORTED);
   body_kernels.push_back(0);
+  body_names.push_back(name);
   return (int)body_kernels.size() - 1;
 }
 
@@ -149,7 +151,10 @@ void Ctx::flush_graph_counts() {
   BSGPU_CUDA(cudaMemsetAsync(d_exec.p, 0, nb * sizeof(unsigned int), st));
   BSGPU_CUDA(cudaStreamSynchronize(st));
   long long n = 0;
-  for (size_t b = 1; b < nb; ++b) n += body_kernels[b] * (long long)h_exec[b];
+  for (size_t b = 1; b < nb; ++b) {
+    n += body_kernels[b] * (long long)h_exec[b];
+    graph_counts[body_names[b]] += h_exec[b];
+  }
   add_launches(n);
   check_graph_errors();
 }
@@ -380,6 +385,85 @@ struct ILU0T : Solver<T> {
     copy_vec(X, B, M->N, c.st);
     if (cnt[1]) gs_update_rows(*M, uinv.p, T(1), rows[1].p, cnt[1], B, X, c.st);
     if (cnt[0]) gs_update_rows(*M, uinv.p, T(1), rows[0].p, cnt[0], B, X, c.st);
+    this->this_level_iterations++;
+    this->converged = true;
+  }
+};
+
+// Block ILU(0) smoother in the reference's natural cell order (CellILU.cs:22; ComputeILU :1229-1330, Solve
+// :182-250).  The dependency chain of the natural order is cut into wavefronts (block rows whose lower neighbours
+// all lie in earlier wavefronts; 3n-2 of them on an n^3 Cartesian grid): the factorisation is one launch per
+// wavefront (ilu0_levels), and x = U^{-1} L^{-1} b is one launch per wavefront and pass: the forward pass
+// y_i = b_i - sum_{k<i} L_ik y_k over the wavefronts in order, the backward pass x_i = U_ii^{-1} (y_i - sum_{j>i}
+// U_ij x_j) in reverse order, both as in-place row updates on zero-initialised vectors (rows not yet visited are
+// zero, so the full row product only sees the finished neighbours).  Factors computed in FP64, stored and applied
+// in FP32 for the mixed-precision preconditioner (the reference's single-precision back substitution,
+// CellILU.cs:914).
+template <typename T>
+struct ILUNaturalT : Solver<T> {
+  bool graphable() const override { return true; }
+  std::unique_ptr<Matrix> M64, M32;
+  const Matrix* M = nullptr;
+  DBuf<double> uinv64;
+  DBuf<float> uinv32;
+  DBuf<int32_t> rows;
+  std::vector<int64_t> lptr;
+  DBuf<T> y;
+  ILUNaturalT(Ctx& c, const Matrix* A64) {
+    require(A64->uniform && (A64->Np == 4 || A64->Np == 6 || A64->Np == 10 || A64->Np == 20),
+            "natural-order ILU needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
+    const int64_t nb = A64->nb;
+    std::vector<int32_t> lev(nb, 0);
+    int nlev = nb ? 1 : 0;
+    for (int64_t i = 0; i < nb; ++i) {
+      for (int64_t k = A64->h_rp[i]; k < A64->h_rp[i + 1]; ++k) {
+        const int32_t j = A64->h_ci[k];
+        if (j < i) lev[i] = std::max(lev[i], lev[j] + 1);
+      }
+      nlev = std::max(nlev, lev[i] + 1);
+    }
+    lptr.assign(nlev + 1, 0);
+    for (int64_t i = 0; i < nb; ++i) lptr[lev[i] + 1]++;
+    for (int l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];
+    std::vector<int32_t> order(nb);
+    std::vector<int64_t> fillp(lptr.begin(), lptr.end() - 1);
+    for (int64_t i = 0; i < nb; ++i) order[fillp[lev[i]]++] = (int32_t)i;
+    rows.alloc(std::max<int64_t>(nb, 1));
+    if (nb) BSGPU_CUDA(cudaMemcpy(rows.p, order.data(), nb * 4, cudaMemcpyHostToDevice));
+    const std::vector<int64_t> o = diag_offsets(*A64);
+    uinv64.alloc(std::max<int64_t>(o.back(), 1));
+    if constexpr (sizeof(T) == 4) uinv32.alloc(std::max<int64_t>(o.back(), 1));
+    M64.reset(matrix_like(*A64, false));
+    int* err = c.flag();
+    ilu0_levels(*A64, rows.p, lptr, *M64, uinv64.p, sizeof(T) == 4 ? uinv32.p : nullptr, err, c.st);
+    c.check_flag(err, "ILU: singular pivot block");
+    if constexpr (sizeof(T) == 4) {
+      M32.reset(matrix_to_single(*M64, c.st));
+      BSGPU_CUDA(cudaStreamSynchronize(c.st));
+      M64.reset();
+      uinv64.release();
+      M = M32.get();
+    } else {
+      M = M64.get();
+    }
+    y.alloc(std::max<int64_t>(M->N, 1));
+  }
+  const T* uinv() const {
+    if constexpr (sizeof(T) == 4)
+      return uinv32.p;
+    else
+      return uinv64.p;
+  }
+  int wavefronts() const { return (int)lptr.size() - 1; }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    (void)zero;  // CellILU overwrites X
+    TraceScope ts(c, this->trace);
+    const int L = wavefronts();
+    fill(T(0), y.p, M->N, c.st);
+    for (int l = 0; l < L; ++l) unit_update_rows(*M, rows.p + lptr[l], lptr[l + 1] - lptr[l], B, y.p, c.st);
+    fill(T(0), X, M->N, c.st);
+    for (int l = L - 1; l >= 0; --l)
+      gs_update_rows(*M, uinv(), T(1), rows.p + lptr[l], lptr[l + 1] - lptr[l], y.p, X, c.st);
     this->this_level_iterations++;
     this->converged = true;
   }
@@ -617,7 +701,7 @@ struct PCGT : Solver<T> {
     pcg_init_kernel<<<1, 1, 0, c.st>>>(s, active);
     BSGPU_CHECK_LAUNCH();
     const cudaGraphConditionalHandle h = c.cond_handle();
-    const int body = c.new_body();
+    const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "CG iteration");
     cond_set(h, active, nullptr, nullptr, 0, c.exec_of(body), c.st);
     c.cond_begin(h, cudaGraphCondTypeWhile, body);
     iteration_kernels(c, X);
@@ -864,6 +948,7 @@ struct OrthoT {
   double* d_hbeta = nullptr;  // projection coefficients of the recorded form [nslots]
   double* d_rn = nullptr;     // residual norm after MinimizeResidual
   OrthoState* dev() { return state.p; }
+  std::string tag;  // owner's trace name, for the graph statistics
   void prepare_dev(Ctx& c, int slots) {
     slots = std::max(1, std::min(slots, cap));
     require(slots <= kHistMax, "recorded OrthoMG: history longer than 128", BSGPU_ERR_UNSUPPORTED);
@@ -909,7 +994,7 @@ struct OrthoT {
     cgs_dev(c, true);
     ortho_decide1(state.p, d_proj, c.d_err, c.st);
     const cudaGraphConditionalHandle h = c.cond_handle();
-    const int body = c.new_body();
+    const int body = c.new_body(tag + "second Gram-Schmidt sweep");
     cond_set(h, &state.p->second, nullptr, nullptr, 0, c.exec_of(body), c.st);
     c.cond_begin(h, cudaGraphCondTypeIf, body);
     cgs_dev(c, false);
@@ -1042,6 +1127,7 @@ struct OrthoMGT : Solver<T> {
     return (coarse ? 1 : 0) + (post ? sweeps : 0) + ((pre && (pre_on == nullptr || *pre_on)) ? 1 : 0);
   }
   void prepare_graph(Ctx& c) override {
+    if (this->trace >= 0) ortho.tag = c.trace[this->trace].name + ": ";
     const int per = std::max(1, corrections_per_iteration());
     const long long most = (long long)std::max(1, term.max_iter) * per;
     ortho.prepare_dev(c, (int)std::min<long long>(most, ortho.cap));
@@ -1061,7 +1147,7 @@ struct OrthoMGT : Solver<T> {
                               int cap_eff) {
     OrthoState* st = ortho.dev();
     const cudaGraphConditionalHandle h = c.cond_handle();
-    const int body = c.new_body();
+    const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "correction");
     cond_set(h, &st->active, post_sweep ? &st->cancel : nullptr, post_sweep ? &st->k : nullptr, cap_eff,
              c.exec_of(body), c.st);
     c.cond_begin(h, cudaGraphCondTypeIf, body);
@@ -1103,7 +1189,7 @@ struct OrthoMGT : Solver<T> {
       return;
     }
     const cudaGraphConditionalHandle h = c.cond_handle();
-    const int body = c.new_body();
+    const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "iteration");
     cond_set(h, &st->active, nullptr, nullptr, 0, c.exec_of(body), c.st);
     c.cond_begin(h, cudaGraphCondTypeWhile, body);
     iteration_dev(c, X, B, tp);
@@ -1169,7 +1255,7 @@ struct GridAndDegT : Solver<T> {
     dots(c.red, 1, a, a, sub->N, d_norm, 1, c.st);
     positive_flag(d_norm, nonzero, c.st);
     const cudaGraphConditionalHandle h = c.cond_handle();
-    const int body = c.new_body();
+    const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "coarse correction");
     cond_set(h, nonzero, nullptr, nullptr, 0, c.exec_of(body), c.st);
     c.cond_begin(h, cudaGraphCondTypeIf, body);
     if (zero)
@@ -1210,6 +1296,28 @@ struct AggregationT : Solver<T> {
     this->converged = lower->converged;
     agg_prolong_add(*g, xc.p, X, c.st);
   }
+  // recorded form: the zero-right-hand-side return becomes an IF node
+  int* nonzero = nullptr;
+  bool graphable() const override { return lower && lower->graphable(); }
+  void prepare_graph(Ctx& c) override {
+    if (!nonzero) nonzero = c.flag();
+    lower->prepare_graph(c);
+  }
+  void solve_graph(Ctx& c, T* X, const T* B, bool zero) override {
+    (void)zero;
+    agg_restrict(*g, B, bc.p, c.st);
+    const T* a[1] = {bc.p};
+    dots(c.red, 1, a, a, g->nc, d_norm, 1, c.st);
+    positive_flag(d_norm, nonzero, c.st);
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "aggregation coarse correction");
+    cond_set(h, nonzero, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeIf, body);
+    fill(T(0), xc.p, g->nc, c.st);
+    lower->solve_graph(c, xc.p, bc.p, true);
+    agg_prolong_add(*g, xc.p, X, c.st);
+    c.cond_end();
+  }
 };
 
 // Direct solve of the coarsest level by a dense inverse computed once in FP64 (DirectSolver, DirectSolver.cs:43).
@@ -1235,6 +1343,7 @@ struct DenseDirectT : Solver<T> {
     this->converged = true;
     this->this_level_iterations = 1;
   }
+  bool graphable() const override { return true; }
 };
 
 // Coarse correction through explicit restriction / prolongation matrices (MultigridOperator.Restrict /
@@ -1266,6 +1375,28 @@ struct TransferT : Solver<T> {
     lower->solve(c, xc.p, bc.p, true);
     this->converged = lower->converged;
     csr_spmv(*P, T(1), xc.p, T(1), X, c.st);
+  }
+  // recorded form: the zero-right-hand-side return becomes an IF node
+  int* nonzero = nullptr;
+  bool graphable() const override { return lower && lower->graphable(); }
+  void prepare_graph(Ctx& c) override {
+    if (!nonzero) nonzero = c.flag();
+    lower->prepare_graph(c);
+  }
+  void solve_graph(Ctx& c, T* X, const T* B, bool zero) override {
+    (void)zero;
+    csr_spmv(*R, T(1), B, T(0), bc.p, c.st);
+    const T* a[1] = {bc.p};
+    dots(c.red, 1, a, a, R->rows, d_norm, 1, c.st);
+    positive_flag(d_norm, nonzero, c.st);
+    const cudaGraphConditionalHandle h = c.cond_handle();
+    const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "transfer coarse correction");
+    cond_set(h, nonzero, nullptr, nullptr, 0, c.exec_of(body), c.st);
+    c.cond_begin(h, cudaGraphCondTypeIf, body);
+    fill(T(0), xc.p, P->cols, c.st);
+    lower->solve_graph(c, xc.p, bc.p, true);
+    csr_spmv(*P, T(1), xc.p, T(1), X, c.st);
+    c.cond_end();
   }
 };
 
@@ -1901,6 +2032,9 @@ std::unique_ptr<Solver<T>> make_smoother(Ctx& c, const Matrix* A64, const Matrix
   } else if (kind == BSGPU_SMOOTHER_ILU) {
     s = std::make_unique<ILU0T<T>>(c, A64);
     tag = ".CellILU";
+  } else if (kind == BSGPU_SMOOTHER_ILU_NATURAL) {
+    s = std::make_unique<ILUNaturalT<T>>(c, A64);
+    tag = ".CellILU";
   } else {
     s = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
   }
@@ -2194,6 +2328,7 @@ double train_learned(Tree& t, int n_rhs, int steps, double lr, uint64_t seed) {
     }
   }
   BSGPU_CUDA(cudaStreamSynchronize(c.st));
+  learned_check(*t.net, c.st);
   t.net->trained = true;
   t.learned_on = true;
   (void)was_on;

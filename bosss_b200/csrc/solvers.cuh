@@ -3,6 +3,7 @@
 // CUDA stream; scalars (norms, projection coefficients) stay in device memory and the host reads back only the
 // values its control flow branches on.
 #pragma once
+#include <map>
 #include <memory>
 
 #include "aggregation.cuh"
@@ -74,7 +75,9 @@ struct Ctx {
   void graph_init();
   void capture_begin();
   long long capture_end(cudaGraph_t* g);  // returns the kernels recorded at the top level
-  int new_body();
+  int new_body(const std::string& name);
+  std::vector<std::string> body_names;
+  std::map<std::string, unsigned long long> graph_counts;  // executions of the conditional bodies, by name
   unsigned int* exec_of(int body) { return d_exec.p + body; }
   cudaGraphConditionalHandle cond_handle();
   void cond_begin(cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, int body);

@@ -234,10 +234,11 @@ class IterativeSolverConfig:
 class PmgConfig(IterativeSolverConfig):
     """PmgConfig.CreateInstanceImpl__Kummer (PmgConfig.cs:80-245).
 
-    Post-smoother of every p-level: ``UseILU = True`` selects block ILU(0) (CellILU, as PmgConfig.cs:124-141 does
-    for the levels it creates; here the cells are ordered by the two colours of the block graph), otherwise
-    ``Smoother``: "blockjacobi" (BlockJacobi with ``BlockJacobiIterations``), "blockgs" (symmetric multicolour
-    block Gauss-Seidel), "schwarz" (restricted additive Schwarz, one patch per cell) or "ilu".
+    Post-smoother of every p-level: ``UseILU = True`` selects block ILU(0) in the natural cell order (CellILU, as
+    PmgConfig.cs:124-141 does for the levels it creates), otherwise ``Smoother``: "blockjacobi" (BlockJacobi with
+    ``BlockJacobiIterations``), "blockgs" (symmetric multicolour block Gauss-Seidel), "schwarz" (restricted
+    additive Schwarz, one patch per cell), "ilu_natural" or "ilu" (block ILU(0) with the cells ordered by the two
+    colours of the block graph).
 
     ``DegreeHierarchy``: modes per species kept on each level, finest first (e.g. (20, 10, 4) for p = 3 -> 2 -> 1
     in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative), by CG
@@ -289,10 +290,10 @@ class PmgConfig(IterativeSolverConfig):
         c.h_cycle = self.HCycle
         c.dense_limit = self.DenseLimit
         sm = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "blockgs": nat.SMOOTHER_BLOCKGS,
-              "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU}
+              "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU, "ilu_natural": nat.SMOOTHER_ILU_NATURAL}
         if self.Smoother not in sm or self.HSmoother not in sm:
             raise ValueError(f"Smoother / HSmoother must be one of {sorted(sm)}")
-        c.smoother = nat.SMOOTHER_ILU if self.UseILU else sm[self.Smoother]
+        c.smoother = nat.SMOOTHER_ILU_NATURAL if self.UseILU else sm[self.Smoother]
         c.h_smoother = sm[self.HSmoother]
         if self.OrthoMaxKrylovDim < 2:
             raise ValueError("OrthoMaxKrylovDim must be at least 2")
@@ -413,17 +414,22 @@ class BlockJacobiConfig:
 class CellILUConfig:
     """CellILU (CellILU.cs:22) with ILU_level = 0 as a stand-alone solver: X = U^{-1} L^{-1} B per call.
 
-    The block ILU(0) factors are computed for the cells ordered by the two colours of the block graph (the
-    reference uses the natural order); blocks must be uniform of size 4, 6, 10 or 20."""
+    ``Order``: "natural" (the reference's cell order, factored and applied wavefront by wavefront) or "coloured"
+    (the cells ordered by the two colours of the block graph: one launch per triangular solve, a different ILU(0)).
+    Blocks must be uniform of size 4, 6, 10 or 20."""
     ILU_level: int = 0
+    Order: str = "natural"
 
     def CreateInstance(self, op: MultigridOperator) -> "GpuSolver":
         if self.ILU_level != 0:
             raise NotImplementedError("only ILU_level = 0 is available")
+        orders = {"natural": nat.SMOOTHER_ILU_NATURAL, "coloured": nat.SMOOTHER_ILU}
+        if self.Order not in orders:
+            raise ValueError(f"Order must be one of {sorted(orders)}")
         c = nat.SolverConfig()
         nat.check(nat.lib().bsgpu_solver_config_default(C.byref(c)))
         c.solver = nat.SOLVER_BLOCKJACOBI
-        c.smoother = nat.SMOOTHER_ILU
+        c.smoother = orders[self.Order]
         return GpuSolver(op, c)
 
 

@@ -147,8 +147,11 @@ enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in 
  * restricted additive Schwarz with one overlapping block per cell (Schwarz.cs:56; bj_iters + 1 updates; blocks
  * of up to ~160 unknowns, uneven sizes allowed), factors in FP32 for the mixed-precision preconditioner */
 enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1, BSGPU_SMOOTHER_SCHWARZ = 2,
-       BSGPU_SMOOTHER_ILU = 3 /* block ILU(0) (CellILU.cs:22, PmgConfig UseILU), cells ordered by the two colours
-                                 of the block graph; uniform blocks of 4, 6, 10 or 20 */ };
+       BSGPU_SMOOTHER_ILU = 3 /* block ILU(0) (CellILU.cs:22), cells ordered by the two colours of the block graph
+                                 (one launch per triangular solve); uniform blocks of 4, 6, 10 or 20 */,
+       BSGPU_SMOOTHER_ILU_NATURAL = 4 /* block ILU(0) in the reference's natural cell order (CellILU.cs:1229-1330,
+                                         PmgConfig UseILU), factored and applied wavefront by wavefront; uniform
+                                         blocks of 4, 6, 10 or 20 */ };
 /* learned preconditioner stage (no counterpart in the reference): a one-hop message-passing MLP over the cell
  * graph, BF16 weights, FP32 accumulation.  FGMRES: an extra FlexGMRES preconditioner used in turn with the
  * p-multigrid V-cycle (FlexGMRES.cs:196-199 round-robin); PRESMOOTH: pre-smoother of the finest OrthoMG level

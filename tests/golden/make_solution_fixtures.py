@@ -1,20 +1,24 @@
 """Solution fixtures of the configured workloads, computed by the oracle (the CPU restatement, FP64).
 
 For every case the oracle solves the DiagBlockEquilib-transformed system (the operator the solvers see) with
-FlexGMRES(30) + p-multigrid to a relative residual far below the solvers' 1e-10, the solution is mapped back to the
-original basis (X = L^T X~), and the file keeps what a GPU test needs to compare a solution of the full system
-without shipping it: the L2 norm, a seeded sample of 10,000 entries (indices and values), the iteration count and
-the residual reached.  The right-hand side is scaled before the solve so that the relative tolerance stays above
-the absolute floor 2.2e-13 of DefaultTermination (IterativeSolverConfig.cs:48-62); the solution is scaled back.
+FlexGMRES(30) + p-multigrid to a relative residual of 1e-12 (the solvers stop at 1e-10), the solution is mapped
+back to the original basis (X = L^T X~), and the file keeps what a GPU test needs to compare a solution of the full
+system without shipping it: the L2 norm, a seeded sample of 10,000 entries (indices and values), the iteration count
+and the residual reached.  The right-hand side is scaled before the solve so that the relative tolerance stays
+above the absolute floor 2.2e-13 of DefaultTermination (IterativeSolverConfig.cs:48-62); the solution is scaled
+back.
 
 The default case also records the outer iteration count and time of the oracle at the benchmark's own settings
 (tolerance 1e-10 and every SOLVER_PARAMS entry of bench.py, RecalcResiPeriod included) in c2_oracle_solve.json:
 the reference arm of bench.py multiplies its per-iteration sample by that count.
 
-    python tests/golden/make_solution_fixtures.py c2 [c1 c3 c4s c4]
+    python tests/golden/make_solution_fixtures.py c2 [c1 c3 c4s c4] [--recount]
+
+(--recount: solve the default case at the benchmark's settings again even if c2_oracle_solve.json holds them.)
 
 Cases: c1 = 2-D 64^2 p=2 (direct solve), c2 = 3-D 64^3 p=3, c3 = XDG sphere 48^3 p=2 (jump 1:1000),
-c4s = variable coefficient 32^3 p=2, c4 = variable coefficient 96^3 p=2.  c2 takes ~30 min, c4 ~1 h on 8 cores.
+c4s = variable coefficient 32^3 p=2, c4 = variable coefficient 96^3 p=2.  Each full-size case takes tens of
+minutes on 8 cores.
 """
 import json
 import os
@@ -76,7 +80,7 @@ def system(case):
     raise ValueError(case)
 
 
-def oracle_krylov(s, levels, tol, scale_to=1e4, **kw):
+def oracle_krylov(s, levels, tol, scale_to=1e4, max_iter=600, **kw):
     """FGMRES + p-MG on the transformed system; returns (X in the original basis, result, seconds)."""
     Bs = O.Bsr.of(s)
     vals, L = O.change_of_basis(Bs)
@@ -88,7 +92,7 @@ def oracle_krylov(s, levels, tol, scale_to=1e4, **kw):
     bt = apply_blocks(L, np.asarray(s.rhs, np.float64), lens, transpose=False)
     scale = scale_to / np.linalg.norm(bt) if scale_to else 1.0
     cfg = O.SolverConfig(solver=O.FGMRES_PMG, tol=tol, top_mode=O.TERM_RELATIVE, level_keep=levels,
-                         coarse_kind=O.COARSE_PCG, max_iter=600, **kw)
+                         coarse_kind=O.COARSE_PCG, max_iter=max_iter, **kw)
     ps = O.PersistentSolver(O.Bsr.of(T), cfg)
     t0 = time.perf_counter()
     r = ps.solve(bt * scale)
@@ -111,7 +115,7 @@ def write_solution(case, x, info):
     print(case, info, flush=True)
 
 
-def main(cases):
+def main(cases, recount=False):
     threads = O.set_threads(os.cpu_count() or 1)
     from bench import SOLVER_PARAMS, TOL
     bench_kw = dict(coarse_tol=SOLVER_PARAMS["CoarseTolerance"], coarse_max_iter=SOLVER_PARAMS["CoarseMaxIterations"],
@@ -126,7 +130,9 @@ def main(cases):
             write_solution(case, x, {"method": "FP64 SuperLU direct solve with 2 refinement steps",
                                      "seconds": time.perf_counter() - t0, "N": int(s.N)})
             continue
-        if case == "c2":
+        count_file = os.path.join(HERE, "c2_oracle_solve.json")
+        have = os.path.exists(count_file) and json.load(open(count_file)).get("settings") == SOLVER_PARAMS
+        if case == "c2" and (recount or not have):
             # the benchmark's own settings, from a zero guess to 1e-10: the reference arm's iteration count
             _, r, dt = oracle_krylov(s, levels, TOL, scale_to=None, **bench_kw)
             out = {"iterations": r.iterations, "converged": r.converged, "seconds": dt, "threads": threads,
@@ -135,8 +141,10 @@ def main(cases):
             with open(os.path.join(HERE, "c2_oracle_solve.json"), "w") as f:
                 json.dump(out, f, indent=1)
             print(out, flush=True)
-        tol = 1e-13
-        x, r, dt = oracle_krylov(s, levels, tol, **bench_kw)
+        # 1e-12 relative (three orders below the solvers' tolerance); the iteration limit keeps the run bounded
+        # where FP64 rounding stops the residual short of it (the fixture records what was reached)
+        tol = 1e-12
+        x, r, dt = oracle_krylov(s, levels, tol, max_iter=40, **bench_kw)
         write_solution(case, x, {"method": f"oracle FlexGMRES(30) + p-MG {levels}, FP64, block-Jacobi smoothing",
                                  "tol_relative": tol, "relres_transformed": r.res / r.res0,
                                  "iterations": r.iterations, "converged": r.converged, "seconds": dt,
@@ -144,4 +152,5 @@ def main(cases):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["c2"])
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    main(args or ["c2"], recount="--recount" in sys.argv)

@@ -13,7 +13,7 @@ def test_fgmres_pmg_fields_reach_the_c_struct():
     assert c.solver == nat.SOLVER_FGMRES_PMG and c.termination == nat.TERM_RELATIVE and c.tol == 1e-9
     assert c.max_krylov == 25 and c.n_levels == 3 and list(c.level_keep)[:3] == [20, 10, 4]
     assert c.post_sweeps == 7 and c.coarse_tol == 0.1 and c.coarse_max_iter == 60
-    assert c.smoother == nat.SMOOTHER_ILU and c.precision == nat.PRECISION_MIXED
+    assert c.smoother == nat.SMOOTHER_ILU_NATURAL and c.precision == nat.PRECISION_MIXED
     assert c.learned == nat.LEARNED_BOTH and c.learned_stall == 0.8
     assert c.ortho_max_krylov == 48 and c.recalc_resi_period == 40
 

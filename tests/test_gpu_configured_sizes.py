@@ -1,7 +1,7 @@
 """GPU solutions of the configured workloads at their full sizes, against the oracle.
 
 The fixtures in tests/golden/*_solution.npz hold, for each full-size system, the oracle's FP64 solution (the CPU
-restatement's FlexGMRES + p-multigrid to a relative residual of 1e-13, or an FP64 direct solve for the 2-D case)
+restatement's FlexGMRES + p-multigrid to a relative residual of 1e-12, or an FP64 direct solve for the 2-D case)
 as its L2 norm and a seeded sample of 10,000 entries; tests/golden/make_solution_fixtures.py wrote them.  Each test
 assembles the same seeded system, solves it on the GPU through the C ABI with the benchmark's settings, and
 compares: relative L2 difference on the sample and of the norm.
