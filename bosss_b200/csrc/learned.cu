@@ -101,7 +101,7 @@ __device__ __forceinline__ void fence_proxy() { asm volatile("fence.proxy.async.
 
 // bounded wait on an mbarrier phase
 __device__ __forceinline__ bool wait_phase(uint32_t mbar, uint32_t parity) {
-  for (long long it = 0; it < (1ll << 26); ++it) {
+  for (long long it = 0; it < (1ll << 22); ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
