@@ -368,6 +368,7 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->learned_pairs = 0;
     cfg->graph = 0;
     cfg->autotune = 0;
+    cfg->fp16_storage = 0;
   });
 }
 

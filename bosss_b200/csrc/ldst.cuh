@@ -4,6 +4,7 @@
 // allocation and with an L2 evict-first policy; that keeps the reused operand (the x vector, about 42 MB for
 // 5.2M unknowns) resident in the 126 MB L2 while several GB of blocks stream past it.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -17,6 +18,9 @@ template <> struct Vec<double, 2> { double a[2]; };
 template <> struct Vec<float, 1> { float a[1]; };
 template <> struct Vec<float, 2> { float a[2]; };
 template <> struct Vec<float, 4> { float a[4]; };
+template <> struct __align__(4) Vec<__half, 2> { __half a[2]; };
+template <> struct __align__(8) Vec<__half, 4> { __half a[4]; };
+template <> struct __align__(16) Vec<__half, 8> { __half a[8]; };
 
 __device__ __forceinline__ uint64_t policy_evict_first() {
   uint64_t p;
@@ -54,6 +58,44 @@ __device__ __forceinline__ Vec<float, 4> ld_stream(const float* ptr, uint64_t po
                : "=f"(v.a[0]), "=f"(v.a[1]), "=f"(v.a[2]), "=f"(v.a[3]) : "l"(ptr), "l"(pol));
   return v;
 }
+
+// FP16 values (matrices of the preconditioner stored in half precision): 2, 4 or 8 halves in one 4-, 8- or
+// 16-byte load, same cache policy
+__device__ __forceinline__ Vec<__half, 2> ld_stream(const __half* ptr, uint64_t pol, Vec<__half, 2>*) {
+  Vec<__half, 2> v;
+  uint32_t r;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(r) : "l"(ptr), "l"(pol));
+  *reinterpret_cast<uint32_t*>(v.a) = r;
+  return v;
+}
+__device__ __forceinline__ Vec<__half, 4> ld_stream(const __half* ptr, uint64_t pol, Vec<__half, 4>*) {
+  Vec<__half, 4> v;
+  uint32_t r0, r1;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.b32 {%0, %1}, [%2], %3;"
+               : "=r"(r0), "=r"(r1) : "l"(ptr), "l"(pol));
+  reinterpret_cast<uint32_t*>(v.a)[0] = r0;
+  reinterpret_cast<uint32_t*>(v.a)[1] = r1;
+  return v;
+}
+__device__ __forceinline__ Vec<__half, 8> ld_stream(const __half* ptr, uint64_t pol, Vec<__half, 8>*) {
+  Vec<__half, 8> v;
+  uint32_t r0, r1, r2, r3;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.b32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3) : "l"(ptr), "l"(pol));
+  reinterpret_cast<uint32_t*>(v.a)[0] = r0;
+  reinterpret_cast<uint32_t*>(v.a)[1] = r1;
+  reinterpret_cast<uint32_t*>(v.a)[2] = r2;
+  reinterpret_cast<uint32_t*>(v.a)[3] = r3;
+  return v;
+}
+
+// widening of a stored value to the arithmetic type
+template <typename T>
+__device__ __forceinline__ T widen(double v) { return (T)v; }
+template <typename T>
+__device__ __forceinline__ T widen(float v) { return (T)v; }
+template <typename T>
+__device__ __forceinline__ T widen(__half v) { return (T)__half2float(v); }
 
 template <typename T, int V>
 __device__ __forceinline__ Vec<T, V> ldv_stream(const T* ptr, uint64_t pol) {

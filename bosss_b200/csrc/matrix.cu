@@ -96,9 +96,9 @@ struct Acc { using type = T; };
 // Uniform Np x Np blocks, Np known at compile time.  A CTA owns BPC = blockDim/NP whole block rows; thread t is DOF
 // row r = t % NP of block row t / NP.  MODE 0: y = alpha*A*x + beta*z.  MODE 1: fused block-Jacobi update
 // y = x + alpha * Dinv * (z - A*x) (z = b), the block row's residual exchanged through shared memory.
-template <typename T, int NP, int V, int MODE>
+template <typename T, int NP, int V, int MODE, typename S = T>
 __global__ void __launch_bounds__(256) spmv_uniform_kernel(
-    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const T* __restrict__ vals,
+    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const S* __restrict__ vals,
     const T* x, const T* __restrict__ z, T* y, T alpha, T beta, int64_t nb,
     const T* __restrict__ dinv, const int* __restrict__ active, const int32_t* __restrict__ row_list = nullptr) {
   static_assert(NP % V == 0, "chunk width must divide the block size");
@@ -121,18 +121,18 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
     const int64_t k0 = rp[i], k1 = rp[i + 1];
     for (int64_t k = k0; k < k1; ++k) {
       const int64_t j = ci[k];
-      const T* vb = vals + k * (NP * NP) + r * V;
+      const S* vb = vals + k * (NP * NP) + r * V;
       const T* xb = x + j * NP;
 #pragma unroll
       for (int c = 0; c < NP / V; ++c) {
-        Vec<T, V> a = ldv_stream<T, V>(vb + c * (NP * V), pol);
+        Vec<S, V> a = ldv_stream<S, V>(vb + c * (NP * V), pol);
         Vec<T, V> xv = ldv_cached<T, V>(xb + c * V);
 #pragma unroll
         for (int q = 0; q < V; ++q) {
           if ((c * V + q) & 1)
-            acc1 = fma(a.a[q], xv.a[q], acc1);
+            acc1 = fma(widen<T>(a.a[q]), xv.a[q], acc1);
           else
-            acc0 = fma(a.a[q], xv.a[q], acc0);
+            acc0 = fma(widen<T>(a.a[q]), xv.a[q], acc0);
         }
       }
     }
@@ -464,15 +464,30 @@ bool specialised(const Matrix& A) {
   }
 }
 
-template <typename T, int NP, int V, int MODE>
-void launch_uniform(const Matrix& A, const T* vals, const T* x, const T* z, T* y, T alpha, T beta, const T* dinv,
+template <typename T, int NP, int V, int MODE, typename S = T>
+void launch_uniform(const Matrix& A, const S* vals, const T* x, const T* z, T* y, T alpha, T beta, const T* dinv,
                     cudaStream_t st, const int* active) {
   const int BPC = std::max(1, A.cta[MODE == 1 ? 1 : 0] / NP);
   const int64_t grid = (A.nb + BPC - 1) / BPC;
   if (grid == 0) return;
-  spmv_uniform_kernel<T, NP, V, MODE><<<(unsigned)grid, BPC * NP, 0, st>>>(A.rp.p, A.ci.p, vals, x, z, y, alpha, beta,
-                                                                          A.nb, dinv, active);
+  spmv_uniform_kernel<T, NP, V, MODE, S><<<(unsigned)grid, BPC * NP, 0, st>>>(A.rp.p, A.ci.p, vals, x, z, y, alpha,
+                                                                             beta, A.nb, dinv, active);
   BSGPU_CHECK_LAUNCH();
+}
+
+// FP16 values, FP32 vectors and arithmetic (the preconditioner's level matrices stored in half precision); uniform
+// blocks of 4, 10 or 20 with the chunk width of the half layout
+template <int MODE>
+void dispatch_half(const Matrix& A, const float* x, const float* z, float* y, float alpha, float beta,
+                   const float* dinv, cudaStream_t st, const int* active) {
+  const __half* v = A.v16.p;
+  if (A.uniform && A.Np == 20 && A.V == 4)
+    return launch_uniform<float, 20, 4, MODE, __half>(A, v, x, z, y, alpha, beta, dinv, st, active);
+  if (A.uniform && A.Np == 10 && A.V == 2)
+    return launch_uniform<float, 10, 2, MODE, __half>(A, v, x, z, y, alpha, beta, dinv, st, active);
+  if (A.uniform && A.Np == 4 && A.V == 4)
+    return launch_uniform<float, 4, 4, MODE, __half>(A, v, x, z, y, alpha, beta, dinv, st, active);
+  throw Error(BSGPU_ERR_UNSUPPORTED, "FP16 matrices: uniform blocks of 4, 10 or 20 only");
 }
 
 template <typename T, int V, int MODE>
@@ -667,6 +682,33 @@ Matrix* matrix_to_single(const Matrix& A, cudaStream_t st) {
   return M.release();
 }
 
+Matrix* matrix_to_half(const Matrix& A, cudaStream_t st) {
+  require(!A.single, "the FP16 copy is made from the FP64 matrix");
+  require(A.uniform && (A.Np == 4 || A.Np == 10 || A.Np == 20), "FP16 matrices: uniform blocks of 4, 10 or 20 only",
+          BSGPU_ERR_UNSUPPORTED);
+  auto M = std::make_unique<Matrix>();
+  M->Np = A.Np;
+  M->uniform = true;
+  M->single = true;
+  M->half = true;
+  M->h_rp = A.h_rp;
+  M->h_ci = A.h_ci;
+  M->h_len = A.h_len;
+  M->h_nspc = A.h_nspc;
+  finish_structure(*M);
+  M->V = A.Np == 10 ? 2 : 4;  // the widest chunk (up to 8 bytes of halves) dividing the block width
+  M->typed = false;
+  M->v16.alloc(std::max<int64_t>(M->nvals, 1));
+  DBuf<int32_t> br = block_rows(A);
+  if (A.nvals) {
+    relayout_kernel<double, __half><<<conv_grid(A.nnzb), 128, 0, st>>>(A.v64.p, A.boff.p, A.V, M->v16.p, M->boff.p,
+                                                                       M->V, br.p, A.ci.p, A.len.p, A.nnzb);
+    BSGPU_CHECK_LAUNCH();
+  }
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  return M.release();
+}
+
 Matrix* matrix_restrict(const Matrix& A, int keep, cudaStream_t st) {
   require(keep >= 1 && keep <= A.Np, "restriction: keep must be in 1..Np");
   auto M = std::make_unique<Matrix>();
@@ -710,6 +752,7 @@ void spmv(const Matrix& A, float alpha, const float* x, float beta, const float*
           const int* active) {
   require(A.single, "FP32 SpMV on an FP64 matrix");
   check_aligned(x, 16, "x");
+  if (A.half) return dispatch_half<0>(A, x, z, y, alpha, beta, nullptr, st, active);
   dispatch<float, 0>(A, A.v32.p, x, z, y, alpha, beta, nullptr, nullptr, st, active);
 }
 
@@ -726,7 +769,8 @@ namespace {
 template <typename T>
 void gs_rows_impl(const Matrix& A, const T* vals, const T* dinv, T omega, const int32_t* rows, int64_t nrows,
                   const T* b, T* x, cudaStream_t st) {
-  require(specialised(A), "block Gauss-Seidel needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
+  require(specialised(A) && !A.half, "block Gauss-Seidel needs uniform blocks of 4, 6, 10 or 20 (FP32/FP64 values)",
+          BSGPU_ERR_UNSUPPORTED);
   if (nrows == 0) return;
   constexpr int VW = sizeof(T) == 8 ? 2 : 4;
 #define BSGPU_GS(NP, VV)                                                                                     \
@@ -753,7 +797,8 @@ namespace {
 template <typename T>
 void unit_rows_impl(const Matrix& A, const T* vals, const int32_t* rows, int64_t nrows, const T* b, T* x,
                     cudaStream_t st) {
-  require(specialised(A), "unit-diagonal row update needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
+  require(specialised(A) && !A.half, "unit-diagonal row update needs uniform blocks of 4, 6, 10 or 20 (FP32/FP64 values)",
+          BSGPU_ERR_UNSUPPORTED);
   if (nrows == 0) return;
   constexpr int VW = sizeof(T) == 8 ? 2 : 4;
 #define BSGPU_UNIT(NP, VV)                                                                                   \
@@ -814,6 +859,10 @@ void bj_update(const Matrix& A, const double* dinv, double omega, const double* 
 void bj_update(const Matrix& A, const float* dinv, float omega, const float* x, const float* b, float* xo,
                cudaStream_t st, const int* active) {
   require(A.single, "precision mismatch");
+  if (A.half) {
+    check_aligned(x, 16, "x");
+    return dispatch_half<1>(A, x, b, xo, omega, 0.0f, dinv, st, active);
+  }
   bj_update_impl<float>(A, A.v32.p, dinv, omega, x, b, xo, st, active);
 }
 
@@ -853,6 +902,15 @@ float time_launches(const Matrix& A, int mode, const T* dinv, const T* x, const 
   BSGPU_CUDA(cudaEventCreate(&e1));
   const T* vals = A.single ? (const T*)(const void*)A.v32.p : (const T*)(const void*)A.v64.p;
   auto one = [&]() {
+    if constexpr (sizeof(T) == 4) {
+      if (A.half) {
+        if (mode == 0)
+          dispatch_half<0>(A, x, nullptr, y, 1.0f, 0.0f, nullptr, st, nullptr);
+        else
+          dispatch_half<1>(A, x, b, y, 1.0f, 0.0f, dinv, st, nullptr);
+        return;
+      }
+    }
     if (mode == 0)
       dispatch<T, 0>(A, vals, x, nullptr, y, T(1), T(0), nullptr, nullptr, st, nullptr);
     else
@@ -872,12 +930,13 @@ float time_launches(const Matrix& A, int mode, const T* dinv, const T* x, const 
 
 template <typename T>
 void autotune_impl(const Matrix& A, int mode, const T* dinv, cudaStream_t st) {
-  const bool tunable = A.typed || specialised(A);
+  const bool tunable = A.typed || specialised(A) || A.half;
   if (!tunable || A.tuned[mode] || A.N == 0) return;
   int dev = 0;
   BSGPU_CUDA(cudaGetDevice(&dev));
   std::ostringstream key;
-  key << dev << (A.typed ? ":typed:" : ":uniform:") << (A.single ? "f32" : "f64") << ":Np" << A.Np << ":V" << A.V
+  key << dev << (A.typed ? ":typed:" : ":uniform:") << (A.half ? "f16" : A.single ? "f32" : "f64") << ":Np" << A.Np
+      << ":V" << A.V
       << ":mode" << mode << ":nb" << A.nb << ":nnzb" << A.nnzb << ":N" << A.N;
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);

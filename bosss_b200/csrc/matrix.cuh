@@ -9,6 +9,8 @@
 // is fully used and no shuffle or shared-memory reduction is needed.  Blocks never straddle a chunk because V
 // divides every block width.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace bsgpu {
@@ -17,7 +19,8 @@ struct Matrix {
   int64_t nb = 0, N = 0, nnzb = 0;
   int Np = 0;            // modes per species
   bool uniform = true;   // every block has Np rows (one species)
-  bool single = false;   // values stored as float
+  bool single = false;   // values stored as float (FP32 arithmetic)
+  bool half = false;     // with single: values stored as FP16 (v16), FP32 arithmetic
   int V = 1;             // chunk width (elements)
   // host copies of the structure
   std::vector<int64_t> h_rp, h_i0;
@@ -41,9 +44,10 @@ struct Matrix {
   int cta_threads = 256;
   DBuf<double> v64;
   DBuf<float> v32;
+  DBuf<__half> v16;
   int64_t nvals = 0;
 
-  size_t value_bytes() const { return (size_t)nvals * (single ? 4 : 8); }
+  size_t value_bytes() const { return (size_t)nvals * (half ? 2 : single ? 4 : 8); }
   int64_t max_len() const;
 };
 
@@ -54,6 +58,9 @@ Matrix* matrix_create(int64_t nb, int32_t Np, const int32_t* nspc, const int64_t
 Matrix* matrix_like(const Matrix& A, bool single);
 void matrix_read_values(const Matrix& A, double* dst, bool dst_device, cudaStream_t st);
 Matrix* matrix_to_single(const Matrix& A, cudaStream_t st);
+// FP16 copy of an FP64 matrix (uniform blocks of 4, 10 or 20) for the preconditioner: products in FP32 arithmetic on
+// half the value traffic.  Marked single (it serves the FP32 kernels' entry points).
+Matrix* matrix_to_half(const Matrix& A, cudaStream_t st);
 Matrix* matrix_restrict(const Matrix& A, int keep, cudaStream_t st);
 
 // y = alpha*A*x + beta*z (z may be y; z == nullptr: beta ignored).  `active`: optional device flag, the launch

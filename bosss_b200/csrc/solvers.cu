@@ -943,6 +943,12 @@ struct OrthoT {
   int nslots = 0;
   DBuf<T> W, MW;
   DBuf<T*> d_sol, d_mxx;
+  // FP16 history of the FP32 preconditioner (entries scaled by hscale = sqrt(N)): half the history traffic
+  bool half_hist = false;
+  float hscale = 1.0f;
+  std::vector<DBuf<__half>> HSol, HMxx;
+  DBuf<__half*> h_sol, h_mxx;
+  bool half() const { return sizeof(T) == 4 && half_hist; }
   DBuf<OrthoState> state;
   HistScratch hs;
   double* d_hbeta = nullptr;  // projection coefficients of the recorded form [nslots]
@@ -953,21 +959,38 @@ struct OrthoT {
     slots = std::max(1, std::min(slots, cap));
     require(slots <= kHistMax, "recorded OrthoMG: history longer than 128", BSGPU_ERR_UNSUPPORTED);
     if (nslots >= slots) return;
-    while ((int)Sol.size() < slots) {
-      Sol.emplace_back(std::max<int64_t>(N, 1));
-      Mxx.emplace_back(std::max<int64_t>(N, 1));
-    }
     W.alloc(std::max<int64_t>(N, 1));
     MW.alloc(std::max<int64_t>(N, 1));
-    std::vector<T*> ps(slots), pm(slots);
-    for (int j = 0; j < slots; ++j) {
-      ps[j] = Sol[j].p;
-      pm[j] = Mxx[j].p;
+    if (half()) {
+      hscale = (float)std::sqrt((double)std::max<int64_t>(N, 1));
+      while ((int)HSol.size() < slots) {
+        HSol.emplace_back(std::max<int64_t>(N, 1));
+        HMxx.emplace_back(std::max<int64_t>(N, 1));
+      }
+      std::vector<__half*> ps(slots), pm(slots);
+      for (int j = 0; j < slots; ++j) {
+        ps[j] = HSol[j].p;
+        pm[j] = HMxx[j].p;
+      }
+      h_sol.alloc(slots);
+      h_mxx.alloc(slots);
+      BSGPU_CUDA(cudaMemcpy(h_sol.p, ps.data(), slots * sizeof(__half*), cudaMemcpyHostToDevice));
+      BSGPU_CUDA(cudaMemcpy(h_mxx.p, pm.data(), slots * sizeof(__half*), cudaMemcpyHostToDevice));
+    } else {
+      while ((int)Sol.size() < slots) {
+        Sol.emplace_back(std::max<int64_t>(N, 1));
+        Mxx.emplace_back(std::max<int64_t>(N, 1));
+      }
+      std::vector<T*> ps(slots), pm(slots);
+      for (int j = 0; j < slots; ++j) {
+        ps[j] = Sol[j].p;
+        pm[j] = Mxx[j].p;
+      }
+      d_sol.alloc(slots);
+      d_mxx.alloc(slots);
+      BSGPU_CUDA(cudaMemcpy(d_sol.p, ps.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
+      BSGPU_CUDA(cudaMemcpy(d_mxx.p, pm.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
     }
-    d_sol.alloc(slots);
-    d_mxx.alloc(slots);
-    BSGPU_CUDA(cudaMemcpy(d_sol.p, ps.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
-    BSGPU_CUDA(cudaMemcpy(d_mxx.p, pm.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
     if (!state.p) {
       state.alloc(1);
       BSGPU_CUDA(cudaMemset(state.p, 0, sizeof(OrthoState)));
@@ -984,6 +1007,15 @@ struct OrthoT {
   // one projection sweep of (W, MW) against the first k history entries; |MW| after it into d_proj[0] and, with
   // `self`, |MW|^2 before it into d_proj[1]
   void cgs_dev(Ctx& c, bool self) {
+    if constexpr (sizeof(T) == 4) {
+      if (half()) {
+        hist_dots(hs, h_mxx.p, &state.p->k, MW.p, N, hscale, d_hbeta, self ? d_proj + 1 : nullptr, c.st);
+        hist_axpy2(h_sol.p, h_mxx.p, &state.p->k, nslots, hscale, d_hbeta, W.p, MW.p, N, c.st);
+        const T* a[1] = {MW.p};
+        dots(c.red, 1, a, a, N, d_proj, 1, c.st);
+        return;
+      }
+    }
     hist_dots(hs, d_mxx.p, &state.p->k, MW.p, N, d_hbeta, self ? d_proj + 1 : nullptr, c.st);
     hist_axpy2(d_sol.p, d_mxx.p, &state.p->k, nslots, d_hbeta, W.p, MW.p, N, c.st);
     const T* a[1] = {MW.p};
@@ -1001,7 +1033,14 @@ struct OrthoT {
     ortho_decide2(state.p, d_proj, c.st);
     c.cond_end();
     ortho_final(state.p, d_proj, c.st);
-    ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
+    if constexpr (sizeof(T) == 4) {
+      if (half())
+        ortho_store(state.p, W.p, MW.p, h_sol.p, h_mxx.p, nslots, hscale, N, c.d_err, c.st);
+      else
+        ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
+    } else {
+      ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
+    }
     ortho_advance(state.p, recalc_period, nslots, c.st);
   }
   void minimize_dev(Ctx& c, T* X, const T* B, const T* Res0, T* Res, const TermParams& tp) {
@@ -1630,6 +1669,20 @@ struct GraphedT : Solver<T> {
     cudaGraphDestroy(g);
     BSGPU_CUDA(e);
   }
+  T* graph_x() { return Xs ? Xs : xin.p; }
+  const T* graph_b() { return Xs ? Bs : bin.p; }
+  // records the graph if there is none yet or the learned pre-smoother was switched since (set-up time)
+  void ensure(Ctx& c) {
+    if (!Xs && !xin.p) {
+      xin.alloc(std::max<int64_t>(N, 1));
+      bin.alloc(std::max<int64_t>(N, 1));
+    }
+    const int k = key_src ? (*key_src ? 1 : 0) : 0;
+    if (!exec || k != key) {
+      capture(c, graph_x(), graph_b());
+      key = k;
+    }
+  }
   void solve(Ctx& c, T* X, const T* B, bool zero) override {
     if (!zero || c.tracing || (Xs && (X != Xs || B != Bs))) {
       inner->solve(c, X, B, zero);
@@ -1637,22 +1690,10 @@ struct GraphedT : Solver<T> {
       this->converged = inner->converged;
       return;
     }
-    T* gx = Xs;
-    const T* gb = Bs;
+    ensure(c);
     if (!Xs) {
-      if (!xin.p) {
-        xin.alloc(std::max<int64_t>(N, 1));
-        bin.alloc(std::max<int64_t>(N, 1));
-      }
-      gx = xin.p;
-      gb = bin.p;
       copy_vec(bin.p, B, N, c.st);
       fill(T(0), xin.p, N, c.st);
-    }
-    const int k = key_src ? (*key_src ? 1 : 0) : 0;
-    if (!exec || k != key) {
-      capture(c, gx, const_cast<T*>(gb));
-      key = k;
     }
     BSGPU_CUDA(cudaGraphLaunch(exec, c.st));
     add_launches(top_kernels);
@@ -1967,7 +2008,10 @@ const Matrix* level_matrix(Tree& t, const Matrix* A64) {
   if constexpr (sizeof(T) == 8) {
     return A64;
   } else {
-    t.owned.emplace_back(matrix_to_single(*A64, t.ctx->st));
+    if (t.cfg.fp16_storage & BSGPU_FP16_MATRICES)
+      t.owned.emplace_back(matrix_to_half(*A64, t.ctx->st));
+    else
+      t.owned.emplace_back(matrix_to_single(*A64, t.ctx->st));
     return t.owned.back().get();
   }
 }
@@ -2004,6 +2048,7 @@ std::unique_ptr<Solver<T>> build_hlevel(Tree& t, const Matrix* A64, const Matrix
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
+  omg->ortho.half_hist = (t.cfg.fp16_storage & BSGPU_FP16_HISTORY) != 0;
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = cfg.h_sweeps;
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -2079,6 +2124,7 @@ std::unique_ptr<Solver<T>> build_hmg_level(Tree& t, const HmgHierarchy* H, const
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
+  omg->ortho.half_hist = (t.cfg.fp16_storage & BSGPU_FP16_HISTORY) != 0;
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = std::max(1, cfg.h_sweeps);
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -2143,6 +2189,7 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
+  omg->ortho.half_hist = (t.cfg.fp16_storage & BSGPU_FP16_HISTORY) != 0;
   omg->trace = c.trace_id(lv + ".OrthoMG");
   if (level == 0 && t.net && (cfg.learned & BSGPU_LEARNED_PRESMOOTH)) {
     omg->pre = std::make_unique<LearnedPrecondT<T>>(c, t.net.get());
@@ -2234,6 +2281,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
           g->Xs = ad->x32.p;
           g->Bs = ad->b32.p;
           g->key_src = &t->learned_on;
+          g->ensure(*t->ctx);  // recorded at set-up, not in the first solve
           ad->inner = std::move(g);
         } else {
           ad->inner = std::move(lvl);
@@ -2246,6 +2294,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
                   BSGPU_ERR_UNSUPPORTED);
           auto g = std::make_unique<GraphedT<double>>(A->N, std::move(lvl));
           g->key_src = &t->learned_on;
+          g->ensure(*t->ctx);  // recorded at set-up, not in the first solve
           f->pc = std::move(g);
         } else {
           f->pc = std::move(lvl);

@@ -269,6 +269,8 @@ class PmgConfig(IterativeSolverConfig):
     OrthoMaxKrylovDim: int = 96     # OrthonormalizationMultigrid.Config.MaxKrylovDim: history length per level
     RecalcResiPeriod: int = 1       # OrthonormalizationMultigrid.RecalcResiPeriod: full residual every n updates
     UseILU: bool = False
+    HistoryFP16: bool = False       # FP16 OrthoMG histories in the recorded FP32 V-cycle (FGMRESConfig Graph + mixed)
+    MatrixFP16: bool = False        # FP16 level matrices in the FP32 V-cycle (FGMRESConfig MixedPrecision)
 
     def _fill(self, c):
         c.n_levels = len(self.DegreeHierarchy)
@@ -301,6 +303,7 @@ class PmgConfig(IterativeSolverConfig):
         if self.RecalcResiPeriod < 1:
             raise ValueError("RecalcResiPeriod must be at least 1")
         c.recalc_resi_period = self.RecalcResiPeriod
+        c.fp16_storage = (nat.FP16_HISTORY if self.HistoryFP16 else 0) | (nat.FP16_MATRICES if self.MatrixFP16 else 0)
 
     def _config(self):
         c = self._base()

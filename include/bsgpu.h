@@ -142,6 +142,10 @@ enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1, BSGPU_COARSE_AMG = 2,
                                OrthoMG to coarse_tol with h_sweeps block-Jacobi sweeps, h_cycle iterations on the
                                coarser h-levels, dense below dense_limit */ };
 enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in FP32, outer FP64 */ };
+/* FP16 storage inside the FP32 preconditioner: OrthoMG histories (with cfg.graph; scaled by sqrt(n), which keeps
+ * a normalised vector's entries in FP16's normal range) and the level matrices (uniform blocks of 4, 10 or 20;
+ * not with the Gauss-Seidel smoother) */
+enum { BSGPU_FP16_HISTORY = 1, BSGPU_FP16_MATRICES = 2 };
 /* post-smoother of the OrthoMG levels: BlockJacobi (BlockJacobi.cs:35; NoOfIterations = bj_iters), symmetric
  * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20), or
  * restricted additive Schwarz with one overlapping block per cell (Schwarz.cs:56; bj_iters + 1 updates; blocks
@@ -198,7 +202,8 @@ typedef struct {
                                on the device, and replay it per application; 0: host-driven (default)       */
   int32_t autotune;         /* 1: pick the launch shape (threads per CTA) of every level matrix's product and
                                block-Jacobi kernels by timing the candidates at set-up (bsgpu_autotune_report) */
-  int32_t reserved[1];
+  int32_t fp16_storage;     /* BSGPU_FP16_* bits, with BSGPU_PRECISION_MIXED: parts of the FP32 preconditioner
+                               stored in FP16, arithmetic staying FP32 (0: none)                     */
 } bsgpu_solver_config;
 
 typedef struct {

@@ -90,3 +90,54 @@ def test_graph_vcycle_rejects_unrecordable_coarse_solver(cuda):
     with pytest.raises(nat.BsgpuError):
         FGMRESConfig(Graph=True, Preconditioners=[PmgConfig(DegreeHierarchy=(4, 1), CoarseSolver="amg")]
                      ).CreateInstance(op)
+
+
+def test_graph_vcycle_fp16_history(cuda):
+    """FP16 OrthoMG histories in the recorded FP32 V-cycle: the same solution, at most two more FGMRES iterations
+    than with FP32 histories."""
+    s = A.poisson_3d(8, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = dict(DegreeHierarchy=(20, 10, 4), CoarseTolerance=0.1, CoarseMaxIterations=60, RecalcResiPeriod=40)
+    ref, _, _ = _solve(op, s, True, True, **pmg)
+    half, xh, _ = _solve(op, s, True, True, HistoryFP16=True, **pmg)
+    xd = O.direct_solve(s)
+    assert half.Converged
+    assert np.linalg.norm(xh - xd) <= SOL_TOL * np.linalg.norm(xd)
+    assert half.ThisLevelIterations <= ref.ThisLevelIterations + 2
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_fp16_level_matrices(cuda, graph):
+    """FP16 level matrices (FP32 arithmetic) in the mixed-precision V-cycle, host-driven and recorded, with FP16
+    histories in the recorded form: the solution to the direct solve's 1e-9, at most two more FGMRES iterations
+    than with FP32 storage."""
+    s = A.poisson_3d(8, 3)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    pmg = dict(DegreeHierarchy=(20, 10, 4), CoarseTolerance=0.1, CoarseMaxIterations=60, RecalcResiPeriod=40)
+    ref, _, _ = _solve(op, s, graph, True, **pmg)
+    half, xh, _ = _solve(op, s, graph, True, MatrixFP16=True, HistoryFP16=graph, **pmg)
+    xd = O.direct_solve(s)
+    assert half.Converged
+    assert np.linalg.norm(xh - xd) <= SOL_TOL * np.linalg.norm(xd)
+    assert half.ThisLevelIterations <= ref.ThisLevelIterations + 2
+
+
+def test_graph_vcycles_in_a_concurrent_batch(cuda):
+    """Independent systems, each with its own recorded V-cycle (recorded at set-up on the calling thread), solved
+    concurrently from host threads: every solution against its direct solve."""
+    from bosss_b200.batch import BatchSolver
+    specs = [dict(n=n, p=1, seed=i, mu=(1.0, 10.0), radius=r, centre=(0.5, 0.48, 0.52))
+             for i, (n, r) in enumerate([(6, 0.3), (8, 0.25), (7, 0.33), (6, 0.2)])]
+    systems = [xdg.xdg_sphere(**sp) for sp in specs]
+    pmg = PmgConfig(DegreeHierarchy=(4, 1), Smoother="schwarz", NoOfPostSmootherSweeps=2, CoarseTolerance=1e-2,
+                    CoarseMaxIterations=200)
+    make = lambda op: {"graph": FGMRESConfig(ConvergenceCriterion=1e-12, termination="relative",
+                                             Preconditioners=[pmg], MixedPrecision=True, Graph=True,
+                                             Autotune=True).CreateInstance(op)}
+    sols = {}
+    out = BatchSolver(make, concurrency=2).run(
+        systems, on_result=lambda name, r, w: sols.__setitem__(r.index, w["X"][name].cpu().numpy()))
+    assert out["graph"].as_dict()["all_converged"]
+    for i, s in enumerate(systems):
+        xd = O.direct_solve(s)
+        assert np.linalg.norm(sols[i] - xd) <= SOL_TOL * np.linalg.norm(xd)
