@@ -369,6 +369,9 @@ BSGPU_API int bsgpu_solver_config_default(bsgpu_solver_config* cfg) {
     cfg->graph = 0;
     cfg->autotune = 0;
     cfg->fp16_storage = 0;
+    cfg->schwarz_parts = 0;
+    cfg->schwarz_overlap = 1;
+    cfg->schwarz_scaling = 0;
   });
 }
 

@@ -503,6 +503,43 @@ struct SchwarzT : Solver<T> {
   }
 };
 
+// Additive Schwarz with multi-cell blocks (Schwarz.cs:56; blocking :190-320, overlap :690-735, Solve :996-1147):
+// per update r = b - A x (skipped from a zero guess, as the reference skips the product for X = 0), x += sum over
+// the blocks of R_b^T A_b^{-1} R_b r, then x *= 1/multiplicity with overlap scaling.  Blocks from
+// schwarz_partition (parts blocks; 0: blocks of 8 cells) grown by `overlap` layers; inverses FP32 in the mixed
+// preconditioner.  bj_iters + 1 updates per call (FixedNoOfIterations), as for the one-cell-patch form.
+template <typename T>
+struct BlockSchwarzT : Solver<T> {
+  bool graphable() const override { return true; }
+  const Matrix* A;
+  std::unique_ptr<SchwarzBlocks> S;
+  DBuf<T> r;
+  int updates;
+  bool scaling;
+  BlockSchwarzT(Ctx& c, const Matrix* A64, const Matrix* AT, int iters, int64_t parts, int overlap, bool scale)
+      : A(AT), updates(iters + 1), scaling(scale && overlap > 0) {
+    auto blocks = schwarz_partition(*A64, parts > 0 ? parts : std::max<int64_t>(1, (A64->nb + 7) / 8));
+    schwarz_extend(*A64, blocks, overlap);
+    int* err = c.flag();
+    S.reset(schwarz_blocks_setup(*A64, blocks, scaling, sizeof(T) == 4, err, c.st));
+    c.check_flag(err, "Schwarz: singular block");
+    r.alloc(std::max<int64_t>(A->N, 1));
+  }
+  void solve(Ctx& c, T* X, const T* B, bool zero) override {
+    TraceScope ts(c, this->trace);
+    if (zero) fill(T(0), X, A->N, c.st);
+    for (int s = 0; s < updates; ++s) {
+      if (s == 0 && zero)
+        copy_vec(r.p, B, A->N, c.st);
+      else
+        spmv(*A, T(-1), X, T(1), B, r.p, c.st);
+      schwarz_blocks_add(*S, r.p, X, c.st);
+      if (scaling) schwarz_blocks_scale(*S, X, c.st);
+    }
+    this->converged = true;
+  }
+};
+
 // ---------------------------------------------------------------------------------------------------------------
 // PCG with a block-diagonal preconditioner (SoftPCG.cs:113-194; also the coarsest-level solve).  The iteration
 // runs on device scalars; its kernels are predicated on a device flag that the convergence test clears, so the
@@ -2080,6 +2117,10 @@ std::unique_ptr<Solver<T>> make_smoother(Ctx& c, const Matrix* A64, const Matrix
   } else if (kind == BSGPU_SMOOTHER_ILU_NATURAL) {
     s = std::make_unique<ILUNaturalT<T>>(c, A64);
     tag = ".CellILU";
+  } else if (kind == BSGPU_SMOOTHER_SCHWARZ_BLOCKS) {
+    s = std::make_unique<BlockSchwarzT<T>>(c, A64, AT, cfg.bj_iters, cfg.schwarz_parts, cfg.schwarz_overlap,
+                                           cfg.schwarz_scaling != 0);
+    tag = ".Schwarz";
   } else {
     s = std::make_unique<BlockJacobiT<T>>(c, A64, AT, cfg.bj_iters, cfg.bj_omega);
   }

@@ -10,6 +10,7 @@
 #include "amg.cuh"
 #include "blas1.cuh"
 #include "blockops.cuh"
+#include "bschwarz.cuh"
 #include "devctl.cuh"
 #include "learned.cuh"
 #include "matrix.cuh"

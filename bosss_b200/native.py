@@ -19,6 +19,7 @@ COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 FP16_HISTORY, FP16_MATRICES = 1, 2
 SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS, SMOOTHER_SCHWARZ, SMOOTHER_ILU, SMOOTHER_ILU_NATURAL = 0, 1, 2, 3, 4
+SMOOTHER_SCHWARZ_BLOCKS = 5
 LEARNED_OFF, LEARNED_FGMRES, LEARNED_PRESMOOTH, LEARNED_BOTH = 0, 1, 2, 3
 
 # every symbol the header declares (checked by the CPU test-suite)
@@ -49,7 +50,9 @@ class SolverConfig(C.Structure):
                 ("dense_limit", C.c_int32), ("smoother", C.c_int32), ("h_smoother", C.c_int32),
                 ("learned", C.c_int32), ("learned_hidden", C.c_int32), ("learned_stall", C.c_double),
                 ("ortho_max_krylov", C.c_int32), ("recalc_resi_period", C.c_int32), ("learned_pairs", C.c_int32),
-                ("graph", C.c_int32), ("autotune", C.c_int32), ("fp16_storage", C.c_int32)]
+                ("graph", C.c_int32), ("autotune", C.c_int32), ("fp16_storage", C.c_int32),
+                ("schwarz_parts", C.c_int32), ("schwarz_overlap", C.c_int32), ("schwarz_scaling", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class SolveStats(C.Structure):

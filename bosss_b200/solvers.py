@@ -237,8 +237,9 @@ class PmgConfig(IterativeSolverConfig):
     Post-smoother of every p-level: ``UseILU = True`` selects block ILU(0) in the natural cell order (CellILU, as
     PmgConfig.cs:124-141 does for the levels it creates), otherwise ``Smoother``: "blockjacobi" (BlockJacobi with
     ``BlockJacobiIterations``), "blockgs" (symmetric multicolour block Gauss-Seidel), "schwarz" (restricted
-    additive Schwarz, one patch per cell), "ilu_natural" or "ilu" (block ILU(0) with the cells ordered by the two
-    colours of the block graph).
+    additive Schwarz, one patch per cell), "schwarz_blocks" (additive Schwarz with multi-cell blocks:
+    ``SchwarzParts``, ``SchwarzOverlap``, ``SchwarzOverlapScaling``), "ilu_natural" or "ilu" (block ILU(0) with the
+    cells ordered by the two colours of the block graph).
 
     ``DegreeHierarchy``: modes per species kept on each level, finest first (e.g. (20, 10, 4) for p = 3 -> 2 -> 1
     in 3-D).  The coarsest level is solved by block-Jacobi PCG to ``CoarseTolerance`` (relative), by CG
@@ -269,6 +270,9 @@ class PmgConfig(IterativeSolverConfig):
     OrthoMaxKrylovDim: int = 96     # OrthonormalizationMultigrid.Config.MaxKrylovDim: history length per level
     RecalcResiPeriod: int = 1       # OrthonormalizationMultigrid.RecalcResiPeriod: full residual every n updates
     UseILU: bool = False
+    SchwarzParts: int = 0           # Smoother "schwarz_blocks": number of blocks (0: blocks of 8 cells)
+    SchwarzOverlap: int = 1         # ... layers of overlap (0, 1, 2)
+    SchwarzOverlapScaling: bool = False
     HistoryFP16: bool = False       # FP16 OrthoMG histories in the recorded FP32 V-cycle (FGMRESConfig Graph + mixed)
     MatrixFP16: bool = False        # FP16 level matrices in the FP32 V-cycle (FGMRESConfig MixedPrecision)
 
@@ -292,7 +296,8 @@ class PmgConfig(IterativeSolverConfig):
         c.h_cycle = self.HCycle
         c.dense_limit = self.DenseLimit
         sm = {"blockjacobi": nat.SMOOTHER_BLOCKJACOBI, "blockgs": nat.SMOOTHER_BLOCKGS,
-              "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU, "ilu_natural": nat.SMOOTHER_ILU_NATURAL}
+              "schwarz": nat.SMOOTHER_SCHWARZ, "ilu": nat.SMOOTHER_ILU, "ilu_natural": nat.SMOOTHER_ILU_NATURAL,
+              "schwarz_blocks": nat.SMOOTHER_SCHWARZ_BLOCKS}
         if self.Smoother not in sm or self.HSmoother not in sm:
             raise ValueError(f"Smoother / HSmoother must be one of {sorted(sm)}")
         c.smoother = nat.SMOOTHER_ILU_NATURAL if self.UseILU else sm[self.Smoother]
@@ -304,6 +309,11 @@ class PmgConfig(IterativeSolverConfig):
             raise ValueError("RecalcResiPeriod must be at least 1")
         c.recalc_resi_period = self.RecalcResiPeriod
         c.fp16_storage = (nat.FP16_HISTORY if self.HistoryFP16 else 0) | (nat.FP16_MATRICES if self.MatrixFP16 else 0)
+        if self.SchwarzOverlap < 0 or self.SchwarzOverlap > 2:
+            raise ValueError("SchwarzOverlap must be 0, 1 or 2")
+        c.schwarz_parts = self.SchwarzParts
+        c.schwarz_overlap = self.SchwarzOverlap
+        c.schwarz_scaling = 1 if self.SchwarzOverlapScaling else 0
 
     def _config(self):
         c = self._base()
@@ -439,24 +449,39 @@ class CellILUConfig:
 @dataclass
 class SchwarzConfig:
     """Schwarz.Config (Schwarz.cs:424) as a stand-alone solver: FixedNoOfIterations (Schwarz.cs:979) updates of
-    restricted additive Schwarz with one block per cell plus its face neighbours (``Overlap`` = 1).
+    additive Schwarz.
 
-    The reference's METIS blocking with ``EnableOverlapScaling`` is replaced by per-cell blocks whose correction is
-    written to the centre cell only (the restricted form), which needs no scaling of the overlap.
+    ``Blocking = "parts"`` (the reference's form): ``NoOfParts`` blocks (METISBlockingStrategy
+    NoOfPartsOnCurrentProcess, Schwarz.cs:195; here a greedy breadth-first partition of the cell graph; 0: blocks of
+    8 cells) grown by ``Overlap`` in {0, 1, 2} layers of neighbours, dense block inverses (at most 1024 unknowns per
+    block), block solutions added, scaled by one over the multiplicity with ``EnableOverlapScaling``.
+    ``Blocking = "cell"``: one block per cell plus its face neighbours with the correction kept on the centre cell
+    (restricted additive Schwarz, Overlap = 1, no scaling): the same sparsity as the operator, applied as one
+    block-sparse product.
     """
     FixedNoOfIterations: int = 1
     Overlap: int = 1
+    Blocking: str = "parts"
+    NoOfParts: int = 0
+    EnableOverlapScaling: bool = False
 
     def CreateInstance(self, op: MultigridOperator) -> "GpuSolver":
-        if self.Overlap != 1:
-            raise NotImplementedError("Schwarz blocks are one cell plus its face neighbours (Overlap = 1)")
         if self.FixedNoOfIterations < 1:
             raise ValueError("FixedNoOfIterations must be at least 1")
+        if self.Overlap < 0 or self.Overlap > 2:
+            raise ValueError("Overlap must be 0, 1 or 2 (Schwarz.cs:501-516)")
+        if self.Blocking not in ("parts", "cell"):
+            raise ValueError("Blocking must be 'parts' or 'cell'")
+        if self.Blocking == "cell" and (self.Overlap != 1 or self.EnableOverlapScaling):
+            raise NotImplementedError("cell blocks are one cell plus its face neighbours (Overlap = 1, no scaling)")
         c = nat.SolverConfig()
         nat.check(nat.lib().bsgpu_solver_config_default(C.byref(c)))
         c.solver = nat.SOLVER_BLOCKJACOBI
-        c.smoother = nat.SMOOTHER_SCHWARZ
+        c.smoother = nat.SMOOTHER_SCHWARZ_BLOCKS if self.Blocking == "parts" else nat.SMOOTHER_SCHWARZ
         c.bj_iters = self.FixedNoOfIterations - 1
+        c.schwarz_parts = self.NoOfParts
+        c.schwarz_overlap = self.Overlap
+        c.schwarz_scaling = 1 if self.EnableOverlapScaling else 0
         return GpuSolver(op, c)
 
 

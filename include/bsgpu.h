@@ -155,7 +155,12 @@ enum { BSGPU_SMOOTHER_BLOCKJACOBI = 0, BSGPU_SMOOTHER_BLOCKGS = 1, BSGPU_SMOOTHE
                                  (one launch per triangular solve); uniform blocks of 4, 6, 10 or 20 */,
        BSGPU_SMOOTHER_ILU_NATURAL = 4 /* block ILU(0) in the reference's natural cell order (CellILU.cs:1229-1330,
                                          PmgConfig UseILU), factored and applied wavefront by wavefront; uniform
-                                         blocks of 4, 6, 10 or 20 */ };
+                                         blocks of 4, 6, 10 or 20 */,
+       BSGPU_SMOOTHER_SCHWARZ_BLOCKS = 5 /* additive Schwarz with multi-cell blocks (Schwarz.cs:56, METIS blocking
+                                            :190-320): cfg.schwarz_parts blocks from a greedy breadth-first
+                                            partition of the cell graph, grown by cfg.schwarz_overlap layers, dense
+                                            block inverses (at most 1024 unknowns per block), optional overlap
+                                            scaling; bj_iters + 1 updates */ };
 /* learned preconditioner stage (no counterpart in the reference): a one-hop message-passing MLP over the cell
  * graph, BF16 weights, FP32 accumulation.  FGMRES: an extra FlexGMRES preconditioner used in turn with the
  * p-multigrid V-cycle (FlexGMRES.cs:196-199 round-robin); PRESMOOTH: pre-smoother of the finest OrthoMG level
@@ -204,6 +209,11 @@ typedef struct {
                                block-Jacobi kernels by timing the candidates at set-up (bsgpu_autotune_report) */
   int32_t fp16_storage;     /* BSGPU_FP16_* bits, with BSGPU_PRECISION_MIXED: parts of the FP32 preconditioner
                                stored in FP16, arithmetic staying FP32 (0: none)                     */
+  int32_t schwarz_parts;    /* BSGPU_SMOOTHER_SCHWARZ_BLOCKS: number of blocks (METISBlockingStrategy
+                               NoOfPartsOnCurrentProcess, Schwarz.cs:195); 0: blocks of 8 cells      */
+  int32_t schwarz_overlap;  /* Schwarz.Config.Overlap (Schwarz.cs:501): 0, 1 (default) or 2 layers   */
+  int32_t schwarz_scaling;  /* Schwarz.Config.EnableOverlapScaling (Schwarz.cs:524): 1 scales by 1/multiplicity */
+  int32_t reserved[5];
 } bsgpu_solver_config;
 
 typedef struct {

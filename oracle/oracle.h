@@ -6,7 +6,8 @@
 enum { OR_OK = 0, OR_ERR_ARGUMENT = 1, OR_ERR_ARITHMETIC = 3 };
 enum { OR_SOLVER_PCG = 0, OR_SOLVER_FGMRES_PMG = 1, OR_SOLVER_ORTHOMG = 2, OR_SOLVER_SOFTGMRES = 3 };
 enum { OR_COARSE_DENSE = 0, OR_COARSE_PCG = 1 };
-enum { OR_SMOOTHER_BLOCKJACOBI = 0, OR_SMOOTHER_SCHWARZ = 1, OR_SMOOTHER_ILU_COLOURED = 2, OR_SMOOTHER_ILU_NATURAL = 3 };
+enum { OR_SMOOTHER_BLOCKJACOBI = 0, OR_SMOOTHER_SCHWARZ = 1, OR_SMOOTHER_ILU_COLOURED = 2, OR_SMOOTHER_ILU_NATURAL = 3,
+       OR_SMOOTHER_SCHWARZ_BLOCKS = 4 };
 
 /* Block-sparse matrix: block i has nspc[i]*Np rows (nspc NULL: 1 species); blocks row-major, concatenated in
  * BSR order (block rows ascending, block columns ascending). */
@@ -37,6 +38,7 @@ typedef struct {
   int32_t reference_fgmres_defect;
   int32_t recalc_resi_period; /* OrthoMG RecalcResiPeriod (OrthonormalizationMultigrid.cs:211); <= 1: every update */
   int32_t smoother;           /* OR_SMOOTHER_*: post-smoother of the p-levels */
+  int32_t schwarz_parts, schwarz_overlap, schwarz_scaling; /* OR_SMOOTHER_SCHWARZ_BLOCKS (0 parts: 8 cells each) */
 } or_solver_cfg;
 
 typedef struct {
@@ -52,6 +54,9 @@ int or_invert(int n, double* A);
 int or_change_of_basis(const or_bsr* m, double* values_out, double* L_out);
 int or_restrict(const or_bsr* m, int keep, double* values_out, int64_t* map_out);
 int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const double* b);
+/* additive Schwarz with multi-cell blocks: `parts` greedy breadth-first blocks (0: 8 cells each) grown by
+ * `overlap` layers, dense block solves, optional overlap scaling; `iters` updates of x */
+int or_block_schwarz(const or_bsr* m, int64_t parts, int overlap, int scaling, int iters, double* x, const double* b);
 int or_schwarz_rows(const or_bsr* m, double* values_out);
 /* block ILU(0) over the block rows in `order` (NULL: natural order); factors in the matrix layout */
 int or_ilu0_factor(const or_bsr* m, const int32_t* order, double* factor_out);

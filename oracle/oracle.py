@@ -18,7 +18,7 @@ _LIB = None
 
 PCG, FGMRES_PMG, ORTHOMG, SOFTGMRES = 0, 1, 2, 3
 COARSE_DENSE, COARSE_PCG = 0, 1
-SMOOTHER_BLOCKJACOBI, SMOOTHER_SCHWARZ, SMOOTHER_ILU_COLOURED, SMOOTHER_ILU_NATURAL = 0, 1, 2, 3
+SMOOTHER_BLOCKJACOBI, SMOOTHER_SCHWARZ, SMOOTHER_ILU_COLOURED, SMOOTHER_ILU_NATURAL, SMOOTHER_SCHWARZ_BLOCKS = 0, 1, 2, 3, 4
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 
 
@@ -33,7 +33,8 @@ class _Cfg(C.Structure):
                 ("level_keep", C.c_int32 * 8), ("post_sweeps", C.c_int32), ("bj_iters", C.c_int32),
                 ("bj_omega", C.c_double), ("coarse_kind", C.c_int32), ("coarse_tol", C.c_double),
                 ("coarse_max_iter", C.c_int32), ("sub_max_iter", C.c_int32), ("sub_reduction", C.c_double),
-                ("reference_fgmres_defect", C.c_int32), ("recalc_resi_period", C.c_int32), ("smoother", C.c_int32)]
+                ("reference_fgmres_defect", C.c_int32), ("recalc_resi_period", C.c_int32), ("smoother", C.c_int32),
+                ("schwarz_parts", C.c_int32), ("schwarz_overlap", C.c_int32), ("schwarz_scaling", C.c_int32)]
 
 
 class _Stats(C.Structure):
@@ -181,6 +182,17 @@ def ilu0_solve(A: Bsr, factor: np.ndarray, b: np.ndarray, order=None) -> np.ndar
     return x
 
 
+def block_schwarz(A: Bsr, x: np.ndarray, b: np.ndarray, parts: int = 0, overlap: int = 1, scaling: bool = False,
+                  iters: int = 1) -> np.ndarray:
+    """Additive Schwarz with multi-cell blocks (Schwarz.cs:56): `iters` updates of x."""
+    x = np.ascontiguousarray(x, np.float64).copy()
+    b = np.ascontiguousarray(b, np.float64)
+    lib().or_block_schwarz.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    _check(lib().or_block_schwarz(C.byref(A._c), int(parts), int(overlap), int(bool(scaling)), int(iters),
+                                  x.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p)))
+    return x
+
+
 def blockjacobi(A: Bsr, x: np.ndarray, b: np.ndarray, iters: int = 1, omega: float = 1.0) -> np.ndarray:
     x = np.ascontiguousarray(x, np.float64).copy()
     b = np.ascontiguousarray(b, np.float64)
@@ -209,6 +221,9 @@ class SolverConfig:
     reference_fgmres_defect: bool = False
     recalc_resi_period: int = 1
     smoother: int = SMOOTHER_BLOCKJACOBI
+    schwarz_parts: int = 0
+    schwarz_overlap: int = 1
+    schwarz_scaling: bool = False
 
     def _c(self) -> _Cfg:
         c = _Cfg()
@@ -223,6 +238,8 @@ class SolverConfig:
         c.reference_fgmres_defect = int(bool(self.reference_fgmres_defect))
         c.recalc_resi_period = int(self.recalc_resi_period)
         c.smoother = int(self.smoother)
+        c.schwarz_parts, c.schwarz_overlap = int(self.schwarz_parts), int(self.schwarz_overlap)
+        c.schwarz_scaling = int(bool(self.schwarz_scaling))
         return c
 
 

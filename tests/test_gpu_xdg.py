@@ -20,7 +20,7 @@ def test_schwarz_block_rows_match_oracle(cuda, Np, spc):
     Bo = O.Bsr.of(v)
     ref = O.spmv(O.Bsr.of(v, values=O.schwarz_rows(Bo)), 1.0, v.rhs, 0.0, np.zeros(v.N))
     op = MultigridOperator(BlockMsrMatrix.from_system(v), MultigridOperator.Eye)
-    sw = SchwarzConfig(FixedNoOfIterations=1).CreateInstance(op)
+    sw = SchwarzConfig(FixedNoOfIterations=1, Blocking="cell").CreateInstance(op)
     x = np.zeros(v.N)
     sw.Solve(x, v.rhs)
     assert np.abs(x - ref).max() <= 1e-10 * np.abs(ref).max()
@@ -38,14 +38,16 @@ def test_schwarz_iterations_match_oracle(cuda):
         x = O.spmv(Mo, 1.0, r, 1.0, x.copy())
     op = MultigridOperator(BlockMsrMatrix.from_system(v), MultigridOperator.Eye)
     got = np.zeros(v.N)
-    SchwarzConfig(FixedNoOfIterations=3).CreateInstance(op).Solve(got, v.rhs)
+    SchwarzConfig(FixedNoOfIterations=3, Blocking="cell").CreateInstance(op).Solve(got, v.rhs)
     assert np.abs(got - x).max() <= 1e-10 * np.abs(x).max()
 
 
 def test_schwarz_rejects_unsupported_overlap(cuda):
     op = MultigridOperator(BlockMsrMatrix.from_system(A.poisson_3d(3, 1)))
     with pytest.raises(NotImplementedError):
-        SchwarzConfig(Overlap=2).CreateInstance(op)
+        SchwarzConfig(Overlap=2, Blocking="cell").CreateInstance(op)
+    with pytest.raises(ValueError):
+        SchwarzConfig(Overlap=3).CreateInstance(op)
 
 
 @pytest.mark.parametrize("mixed", [False, True])
@@ -130,6 +132,6 @@ def test_schwarz_block_covering_everything_is_exact(cuda):
     v = dense_block_system(6, 4, seed=5)
     op = MultigridOperator(BlockMsrMatrix.from_system(v), MultigridOperator.Eye)
     x = np.zeros(v.N)
-    SchwarzConfig(FixedNoOfIterations=1).CreateInstance(op).Solve(x, v.rhs)
+    SchwarzConfig(FixedNoOfIterations=1, Blocking="cell").CreateInstance(op).Solve(x, v.rhs)
     xs = np.linalg.solve(v.to_scipy().toarray(), v.rhs)
     assert np.linalg.norm(x - xs) <= 1e-13 * np.linalg.norm(xs)

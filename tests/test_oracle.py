@@ -315,3 +315,17 @@ def test_natural_order_ilu_parallelises_by_wavefronts():
     b = np.random.default_rng(0).standard_normal(s.N)
     x1, x2 = O.ilu0_solve(Bo, F_nat, b), O.ilu0_solve(Bo, F_wave, b, order)
     assert np.abs(x1 - x2).max() <= 1e-12 * np.abs(x1).max()
+
+
+def test_block_schwarz_single_block_is_exact_and_overlap_sums():
+    """Oracle multi-cell Schwarz: one block covering the system is an exact solve (addSchwarzTest.cs:186-202); with
+    every cell its own block and no overlap it is block Jacobi."""
+    from bosss_b200 import assembly as A
+    s = A.poisson_3d(3, 1, seed=2)
+    Bo = O.Bsr.of(s)
+    x = O.block_schwarz(Bo, np.zeros(s.N), s.rhs, parts=1, overlap=0, iters=1)
+    xs = np.linalg.solve(s.to_scipy().toarray(), s.rhs)
+    assert np.linalg.norm(x - xs) <= 1e-12 * np.linalg.norm(xs)
+    bj = O.block_schwarz(Bo, np.zeros(s.N), s.rhs, parts=s.nb, overlap=0, iters=1)
+    ref = O.blockjacobi(Bo, np.zeros(s.N), s.rhs, iters=0)
+    assert np.linalg.norm(bj - ref) <= 1e-12 * np.linalg.norm(ref)
