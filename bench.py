@@ -32,11 +32,11 @@ METRIC = "time-to-1e-10 residual & iters: learned+mixed vs plain FP64 GPU; SpMV 
 WORKLOAD = "SIP DG Poisson 3-D 64^3 hex, p=3 (Np=20, 5.24M DOF), FlexGMRES(30) + 3-level p-MG (3->2->1), BJ smoothing"
 TOL = 1e-10
 # p-multigrid settings shared by every path (PmgConfig.cs:80-245 with UseILU = false; the coarsest p = 1 level,
-# a direct solve in the reference, is block-Jacobi PCG to 0.1 reduction, at most 60 iterations; the OrthoMG
+# a direct solve in the reference, is block-Jacobi PCG to 0.05 reduction, at most 120 iterations; the OrthoMG
 # residual is recomputed from scratch every 40 updates, the reference's RecalcResiPeriod parameter,
 # OrthonormalizationMultigrid.cs:179-211)
-SOLVER_PARAMS = dict(NoOfPostSmootherSweeps=10, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.1,
-                     CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, RecalcResiPeriod=40)
+SOLVER_PARAMS = dict(NoOfPostSmootherSweeps=10, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.05,
+                     CoarseMaxIterations=120, SubLevelReduction=0.1, SubLevelMaxIterations=100, RecalcResiPeriod=40)
 
 
 def parse():
@@ -64,8 +64,8 @@ def parse():
                     help="fast form without the launch-shape autotuner")
     ap.add_argument("--no-learned-variant", dest="learned_variant", action="store_false",
                     help="default workload: skip the learned-stage variant")
-    ap.add_argument("--fp16", default="both", choices=["none", "history", "matrices", "both"],
-                    help="FP16 storage inside the fast form's FP32 preconditioner")
+    ap.add_argument("--fp16", default="none", choices=["none", "matrices"],
+                    help="FP16 level matrices inside the fast form's FP32 preconditioner (weaker preconditioner)")
     return ap.parse_args()
 
 
@@ -247,7 +247,7 @@ def _reference_iterations(args):
     path = os.path.join(ROOT, "tests", "golden", "c2_oracle_solve.json")
     if os.path.exists(path) and args.n == 64 and args.p == 3 and args.seed == 0:
         d = json.load(open(path))
-        if d.get("settings", {}).get("RecalcResiPeriod") == SOLVER_PARAMS["RecalcResiPeriod"]:
+        if d.get("settings") == SOLVER_PARAMS:
             return int(d["iterations"]), "the CPU restatement's own count on this system at these settings"
     return 9, "assumed equal to the default system's count"
 
@@ -314,8 +314,7 @@ def run_ours(args):
         return
 
     def mk(mixed, graph=False, tune=False, learned="off", fp16="none"):
-        pmg = PmgConfig(DegreeHierarchy=levels_for(args.p), HistoryFP16=fp16 in ("history", "both") and graph,
-                        MatrixFP16=fp16 in ("matrices", "both"), **SOLVER_PARAMS)
+        pmg = PmgConfig(DegreeHierarchy=levels_for(args.p), MatrixFP16=fp16 == "matrices", **SOLVER_PARAMS)
         return FGMRESConfig(ConvergenceCriterion=TOL, termination="relative", MaxKrylovDim=30, Preconditioners=[pmg],
                             MixedPrecision=mixed, Graph=graph, Autotune=tune, Learned=learned,
                             LearnedPairs=200).CreateInstance(op)
@@ -348,37 +347,8 @@ def run_ours(args):
             ts.append(a.elapsed_time(b) * 1e-3)
         return min(ts)
 
-    # the plain FP64 GPU multigrid: the reference's algorithm in FP64, host-driven V-cycle
-    plain, t_setup_plain = timed_setup(lambda: mk(False))
-    plain_t = time_variant(plain)
-    plain_iters = plain.ThisLevelIterations
-    plain_res = _true_relres(Aop, op, X, B, s)
-    x_plain = X.clone()
-    plain.Dispose()
-
-    # other forms, for the attribution of the speed-up (each: set-up, one warm-up, best of two)
-    variants = {}
-    forms = {"fp64_graph": dict(mixed=False, graph=True, tune=args.autotune),
-             "mixed_host": dict(mixed=True)}
-    for name, kw in forms.items():
-        slv, t_set = timed_setup(lambda: mk(**kw))
-        t = time_variant(slv)
-        variants[name] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
-                          "setup_s": t_set, "final_relres": _true_relres(Aop, op, X, B, s)}
-        slv.Dispose()
-    if args.learned_variant:
-        # the learned stage (FGMRES round-robin and pre-smoother) on top of the fast form, trained on 200
-        # residuals the solver generates (the Arnoldi vectors of 5 solves with seeded right-hand sides)
-        op.SetCellGraph(s.grid.face_neighbours())
-        slv, t_set = timed_setup(lambda: mk(True, args.graph, args.autotune, learned="both", fp16=args.fp16))
-        _, t_train = timed_setup(lambda: slv.TrainLearned(n_rhs=5, steps=400, lr=2e-3, seed=1))
-        t = time_variant(slv)
-        variants["learned_mixed"] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
-                                     "setup_s": t_set, "train_s": t_train, "pairs": slv.LearnedInfo()["pairs"],
-                                     "final_relres": _true_relres(Aop, op, X, B, s)}
-        slv.Dispose()
-
-    # the fast form: FP32 preconditioner, V-cycle recorded as one CUDA graph, autotuned launch shapes
+    # 1. the fast form: FP32 preconditioner, V-cycle recorded as one CUDA graph, autotuned launch shapes; timed
+    #    first, so that a profiler's launch window over the NVTX range "timed_fast" starts early
     fast, t_setup_fast = timed_setup(lambda: mk(True, args.graph, args.autotune, fp16=args.fp16))
     for _ in range(args.warmup):
         solve(fast)
@@ -387,7 +357,7 @@ def run_ours(args):
     launches0 = nat.launch_count()
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
-        torch.cuda.nvtx.range_push("timed_fast")  # profilers can restrict a launch list to the timed solves
+        torch.cuda.nvtx.range_push("timed_fast")
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         for _ in range(args.steps):
@@ -401,9 +371,9 @@ def run_ours(args):
     t_fast_max = max_over_ranks(t_fast, ws)
     fast_iters = fast.ThisLevelIterations
     fast_res = _true_relres(Aop, op, X, B, s)
-    sol_diff = (torch.linalg.norm(X - x_plain) / torch.linalg.norm(x_plain)).item()
+    x_fast = X.clone()
 
-    # --- end to end through the public API with host (pinned) buffers
+    # 2. end to end through the public API with host (pinned) buffers
     bh = torch.from_numpy(s.rhs).pin_memory()
     xh = torch.zeros(s.N, dtype=torch.float64).pin_memory()
     bn, xn = bh.numpy(), xh.numpy()
@@ -419,7 +389,42 @@ def run_ours(args):
         if i > 0:
             e2e.append(a.elapsed_time(b) * 1e-3)
     e2e_t = max_over_ranks(sum(e2e) / len(e2e), ws)
+    fast.Dispose()
+
+    # 3. the plain FP64 GPU multigrid: the reference's algorithm in FP64, host-driven V-cycle
+    plain, t_setup_plain = timed_setup(lambda: mk(False))
+    torch.cuda.nvtx.range_push("variant_plain_fp64")
+    plain_t = time_variant(plain)
+    torch.cuda.nvtx.range_pop()
+    plain_iters = plain.ThisLevelIterations
+    plain_res = _true_relres(Aop, op, X, B, s)
+    sol_diff = (torch.linalg.norm(x_fast - X) / torch.linalg.norm(X)).item()
+    plain.Dispose()
     plain_max = max_over_ranks(plain_t, ws)
+
+    # 4. other forms, for the attribution of the speed-up (each: set-up, one warm-up, best of two)
+    variants = {}
+    forms = {"fp64_graph": dict(mixed=False, graph=True, tune=args.autotune),
+             "mixed_host": dict(mixed=True)}
+    for name, kw in forms.items():
+        slv, t_set = timed_setup(lambda: mk(**kw))
+        torch.cuda.nvtx.range_push("variant_" + name)
+        t = time_variant(slv)
+        torch.cuda.nvtx.range_pop()
+        variants[name] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
+                          "setup_s": t_set, "final_relres": _true_relres(Aop, op, X, B, s)}
+        slv.Dispose()
+    if args.learned_variant:
+        # the learned stage (FGMRES round-robin and pre-smoother) on top of the fast form, trained on 200
+        # residuals the solver generates (the Arnoldi vectors of 5 solves with seeded right-hand sides)
+        op.SetCellGraph(s.grid.face_neighbours())
+        slv, t_set = timed_setup(lambda: mk(True, args.graph, args.autotune, learned="both", fp16=args.fp16))
+        _, t_train = timed_setup(lambda: slv.TrainLearned(n_rhs=5, steps=400, lr=2e-3, seed=1))
+        t = time_variant(slv)
+        variants["learned_mixed"] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
+                                     "setup_s": t_set, "train_s": t_train, "pairs": slv.LearnedInfo()["pairs"],
+                                     "final_relres": _true_relres(Aop, op, X, B, s)}
+        slv.Dispose()
 
     clocks = clk.summary()
     if rank != 0:
@@ -509,9 +514,7 @@ XDGBATCH = ("independent XDG sphere problems, edge in {16,24,32,40,48}, p=2, rad
             "{10,100,1000}, FlexGMRES(30) + 3-level p-MG (p=2->1->0)")
 # p-multigrid settings of these workloads: FP32 Schwarz smoothing (4 post-sweeps) for the fast path, the plain
 # FP64 path as in the default workload (block Jacobi, 10 post-sweeps)
-PMG_SCHWARZ = dict(NoOfPostSmootherSweeps=4, BlockJacobiIterations=1, CoarseSolver="pcg", CoarseTolerance=0.1,
-                   CoarseMaxIterations=60, SubLevelReduction=0.1, SubLevelMaxIterations=100, Smoother="schwarz",
-                   RecalcResiPeriod=40)
+PMG_SCHWARZ = dict(SOLVER_PARAMS, NoOfPostSmootherSweeps=4, Smoother="schwarz")
 PMG_BJ = dict(SOLVER_PARAMS, Smoother="blockjacobi")
 
 
@@ -592,8 +595,7 @@ def run_single_system(args, s, workload, prepare=None):
     # forms with the recorded V-cycle, autotuned launch shapes and FP16 storage; the faster of the two mixed forms
     # (plus the learned stage with --learned) is the fast form timed over the K steps
     uniform = getattr(s, "nspc", None) is None or int(np.max(s.nspc)) == 1
-    fp16 = dict(HistoryFP16=args.graph and args.fp16 in ("history", "both"),
-                MatrixFP16=uniform and args.fp16 in ("matrices", "both"))
+    fp16 = dict(MatrixFP16=uniform and args.fp16 == "matrices")
     variants = {"plain_fp64": (PMG_BJ, False, False), "fp64_schwarz": (PMG_SCHWARZ, False, False),
                 "mixed_bj": (dict(PMG_BJ, **fp16), True, True), "mixed_schwarz": (dict(PMG_SCHWARZ, **fp16), True, True)}
     res = {}

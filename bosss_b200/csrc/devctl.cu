@@ -194,179 +194,6 @@ __global__ void __launch_bounds__(kThreads) hist_axpy2_kernel(const T* const* __
   }
 }
 
-// FP16 history (scaled by hscale) against an FP32 vector, 8 elements (one 16-byte load of history) per step.
-__device__ __forceinline__ void h8(const uint4& u, float* f) {
-  const __half2* h = reinterpret_cast<const __half2*>(&u);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float2 v = __half22float2(h[i]);
-    f[2 * i] = v.x;
-    f[2 * i + 1] = v.y;
-  }
-}
-
-__global__ void __launch_bounds__(kThreads) hist_dots_h_kernel(const __half* const* __restrict__ hist,
-                                                               const int* __restrict__ kp, int kmax,
-                                                               const float* __restrict__ m, int64_t n, float inv_scale,
-                                                               double* __restrict__ beta, double* __restrict__ self,
-                                                               double* __restrict__ partial,
-                                                               unsigned int* __restrict__ ticket) {
-  const int k = min(*kp, kmax);
-  const int j0 = blockIdx.y * kChunk;
-  const int K = max(0, min(kChunk, k - j0));
-  const bool do_self = self != nullptr && blockIdx.y == 0;
-  if (K == 0 && !do_self) return;
-  __shared__ const __half* ptr[kChunk];
-  if (threadIdx.x < K) ptr[threadIdx.x] = hist[j0 + threadIdx.x];
-  __syncthreads();
-  double acc[kProducts];
-#pragma unroll
-  for (int q = 0; q < kProducts; ++q) acc[q] = 0.0;
-  const int64_t n8 = n / 8;
-  const int64_t stride = (int64_t)gridDim.x * kThreads;
-  for (int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x; j < n8; j += stride) {
-    const float4 m0 = __ldg(reinterpret_cast<const float4*>(m) + 2 * j);
-    const float4 m1 = __ldg(reinterpret_cast<const float4*>(m) + 2 * j + 1);
-    const float mm[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-#pragma unroll
-    for (int q = 0; q < kChunk; ++q)
-      if (q < K) {
-        float f[8];
-        h8(__ldcs(reinterpret_cast<const uint4*>(ptr[q]) + j), f);
-        float s = 0.0f;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) s = fmaf(f[i], mm[i], s);
-        acc[q] += (double)s;
-      }
-    if (do_self) {
-      float s = 0.0f;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) s = fmaf(mm[i], mm[i], s);
-      acc[kChunk] += (double)s;
-    }
-  }
-  for (int64_t i = n8 * 8 + (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-    const double b = (double)m[i];
-#pragma unroll
-    for (int q = 0; q < kChunk; ++q)
-      if (q < K) acc[q] = fma((double)__half2float(ptr[q][i]), b, acc[q]);
-    if (do_self) acc[kChunk] = fma(b, b, acc[kChunk]);
-  }
-#pragma unroll
-  for (int q = 0; q < kChunk; ++q) acc[q] *= (double)inv_scale;
-  __shared__ double red[kThreads / 32][kProducts];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < kProducts; ++q) {
-    const double v = warp_sum(acc[q]);
-    if (lane == 0) red[warp][q] = v;
-  }
-  __syncthreads();
-  const int64_t G = gridDim.x;
-  double* part = partial + (int64_t)blockIdx.y * kProducts * G;
-  if (threadIdx.x < kProducts) {
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w) s += red[w][threadIdx.x];
-    part[(int64_t)threadIdx.x * G + blockIdx.x] = s;
-  }
-  __threadfence();
-  __syncthreads();
-  __shared__ bool last;
-  if (threadIdx.x == 0) last = (atomicAdd(ticket + blockIdx.y, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  for (int q = warp; q < kProducts; q += kThreads / 32) {
-    const bool wanted = (q < K) || (q == kChunk && do_self);
-    if (!wanted) continue;
-    double s = 0.0;
-    for (int64_t b = lane; b < G; b += 32) s += __ldcg(part + (int64_t)q * G + b);
-    s = warp_sum(s);
-    if (lane == 0) {
-      if (q < K)
-        beta[j0 + q] = s;
-      else
-        *self = s;
-    }
-  }
-  if (threadIdx.x == 0) ticket[blockIdx.y] = 0u;
-}
-
-__global__ void __launch_bounds__(kThreads) hist_axpy2_h_kernel(const __half* const* __restrict__ x1,
-                                                                const __half* const* __restrict__ x2,
-                                                                const int* __restrict__ kp, int kmax, float inv_scale,
-                                                                const double* __restrict__ beta,
-                                                                float* __restrict__ y1, float* __restrict__ y2,
-                                                                int64_t n) {
-  const int k = min(*kp, min(kmax, kHistMax));
-  if (k <= 0) return;
-  __shared__ const __half* p1[kHistMax];
-  __shared__ const __half* p2[kHistMax];
-  __shared__ float c[kHistMax];
-  for (int j = threadIdx.x; j < k; j += kThreads) {
-    p1[j] = x1[j];
-    p2[j] = x2[j];
-    c[j] = (float)(beta[j] * (double)inv_scale);
-  }
-  __syncthreads();
-  const int64_t n8 = n / 8;
-  const int64_t stride = (int64_t)gridDim.x * kThreads;
-  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n8; i += stride) {
-    float a1[8], a2[8];
-#pragma unroll
-    for (int w = 0; w < 8; ++w) a1[w] = a2[w] = 0.0f;
-    for (int j = 0; j < k; ++j) {
-      float u[8], v[8];
-      h8(__ldcs(reinterpret_cast<const uint4*>(p1[j]) + i), u);
-      h8(__ldcs(reinterpret_cast<const uint4*>(p2[j]) + i), v);
-#pragma unroll
-      for (int w = 0; w < 8; ++w) {
-        a1[w] = fmaf(c[j], u[w], a1[w]);
-        a2[w] = fmaf(c[j], v[w], a2[w]);
-      }
-    }
-    float4* o1 = reinterpret_cast<float4*>(y1) + 2 * i;
-    float4* o2 = reinterpret_cast<float4*>(y2) + 2 * i;
-    float4 q0 = o1[0], q1 = o1[1], r0 = o2[0], r1 = o2[1];
-    q0.x -= a1[0]; q0.y -= a1[1]; q0.z -= a1[2]; q0.w -= a1[3];
-    q1.x -= a1[4]; q1.y -= a1[5]; q1.z -= a1[6]; q1.w -= a1[7];
-    r0.x -= a2[0]; r0.y -= a2[1]; r0.z -= a2[2]; r0.w -= a2[3];
-    r1.x -= a2[4]; r1.y -= a2[5]; r1.z -= a2[6]; r1.w -= a2[7];
-    o1[0] = q0; o1[1] = q1; o2[0] = r0; o2[1] = r1;
-  }
-  for (int64_t i = n8 * 8 + (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
-    float a1 = 0.0f, a2 = 0.0f;
-    for (int j = 0; j < k; ++j) {
-      a1 = fmaf(c[j], __half2float(p1[j][i]), a1);
-      a2 = fmaf(c[j], __half2float(p2[j][i]), a2);
-    }
-    y1[i] -= a1;
-    y2[i] -= a2;
-  }
-}
-
-__global__ void ortho_store_h_kernel(const OrthoState* __restrict__ s, float* __restrict__ W, float* __restrict__ MW,
-                                     __half* const* __restrict__ sol, __half* const* __restrict__ mxx, int nslots,
-                                     float hscale, int64_t n, int* __restrict__ err) {
-  const int k = s->k;
-  if (k < 0 || k >= nslots) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, kDevErrSlots);
-    return;
-  }
-  const float f = (float)s->fac;
-  __half* S = sol[k];
-  __half* M = mxx[k];
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float w = W[i] * f;
-    const float mw = MW[i] * f;
-    W[i] = w;
-    MW[i] = mw;
-    S[i] = __float2half_rn(w * hscale);
-    M[i] = __float2half_rn(mw * hscale);
-  }
-}
-
 // After the first projection sweep: the norm of the correction's image before (nM) and after it, relative (rel),
 // and whether a second sweep restores orthogonality (1e-5 < rel < 0.5, "twice is enough"; the cancellation bound
 // 1e-5 of OrthonormalizationMultigrid.cs:263-337).  With an empty history there is nothing to project and rel = 1.
@@ -565,31 +392,6 @@ void hist_axpy2(const double* const* x1, const double* const* x2, const int* k, 
 void hist_axpy2(const float* const* x1, const float* const* x2, const int* k, int kmax, const double* beta, float* y1,
                 float* y2, int64_t n, cudaStream_t st) {
   hist_axpy2_impl<float>(x1, x2, k, kmax, beta, y1, y2, n, st);
-}
-
-void hist_dots(HistScratch& s, const __half* const* hist, const int* k, const float* m, int64_t n, float hscale,
-               double* beta, double* self, cudaStream_t st) {
-  require(s.chunks > 0, "history multi-dot: scratch not initialised");
-  require((reinterpret_cast<uintptr_t>(m) & 15) == 0, "history multi-dot: unaligned vector");
-  const int G = std::min(grid_for(std::max<int64_t>(n / 8, 1)), s.grid);
-  const int kmax = s.chunks * kChunk > s.slots ? s.slots : s.chunks * kChunk;
-  hist_dots_h_kernel<<<dim3(G, s.chunks), kThreads, 0, st>>>(hist, k, kmax, m, n, 1.0f / hscale, beta, self,
-                                                               s.partial.p, s.ticket.p);
-  BSGPU_CHECK_LAUNCH();
-}
-void hist_axpy2(const __half* const* x1, const __half* const* x2, const int* k, int kmax, float hscale,
-                const double* beta, float* y1, float* y2, int64_t n, cudaStream_t st) {
-  require((reinterpret_cast<uintptr_t>(y1) & 15) == 0 && (reinterpret_cast<uintptr_t>(y2) & 15) == 0,
-          "history multi-axpy: unaligned vector");
-  require(kmax >= 1 && kmax <= kHistMax, "history multi-axpy: 1 <= slots <= 128");
-  hist_axpy2_h_kernel<<<grid_for(std::max<int64_t>(n / 8, 1)) * 2, kThreads, 0, st>>>(x1, x2, k, kmax, 1.0f / hscale,
-                                                                                      beta, y1, y2, n);
-  BSGPU_CHECK_LAUNCH();
-}
-void ortho_store(OrthoState* s, float* W, float* MW, __half* const* sol, __half* const* mxx, int nslots, float hscale,
-                 int64_t n, int* err, cudaStream_t st) {
-  ortho_store_h_kernel<<<grid_for(n) * 4, kThreads, 0, st>>>(s, W, MW, sol, mxx, nslots, hscale, n, err);
-  BSGPU_CHECK_LAUNCH();
 }
 
 void ortho_decide1(OrthoState* s, const double* proj, int* err, cudaStream_t st) {

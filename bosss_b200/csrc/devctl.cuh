@@ -9,8 +9,6 @@
 // those kernels set.  The history length is a device counter, so the projections use kernels that read it: one
 // multi-dot launch and one dual multi-axpy launch whatever the history length.
 #pragma once
-#include <cuda_fp16.h>
-
 #include "blas1.cuh"
 
 namespace bsgpu {
@@ -68,15 +66,6 @@ void hist_axpy2(const double* const* x1, const double* const* x2, const int* k, 
                 double* y1, double* y2, int64_t n, cudaStream_t st);
 void hist_axpy2(const float* const* x1, const float* const* x2, const int* k, int kmax, const double* beta, float* y1,
                 float* y2, int64_t n, cudaStream_t st);
-// The same two kernels with the history stored in FP16, scaled by `hscale` (stored h = fp16(v * hscale); the
-// vectors of a normalised history have entries of order 1/sqrt(n), so hscale = sqrt(n) keeps them in FP16's normal
-// range), for the FP32 preconditioner: half the history traffic of the projections.
-void hist_dots(HistScratch& s, const __half* const* hist, const int* k, const float* m, int64_t n, float hscale,
-               double* beta, double* self, cudaStream_t st);
-void hist_axpy2(const __half* const* x1, const __half* const* x2, const int* k, int kmax, float hscale,
-                const double* beta, float* y1, float* y2, int64_t n, cudaStream_t st);
-void ortho_store(OrthoState* s, float* W, float* MW, __half* const* sol, __half* const* mxx, int nslots, float hscale,
-                 int64_t n, int* err, cudaStream_t st);
 // upper bound on the iterations of any recorded loop (a safety bound above every configured limit)
 constexpr int kMaxRecordedIterations = 100000;
 

@@ -272,10 +272,12 @@ __global__ void __launch_bounds__(128) mlp_fwd_tc_kernel(FwdArgs a, const TV* __
       bad = true;
       break;
     }
-    float y[16];
-    tc::ld16(tmem + lane_base, y);
-    if (valid)
-      for (int o = 0; o < a.Np; ++o) z[c * a.Np + o] = (TV)((double)y[o] * sc);
+    for (int cb = 0; cb < Op; cb += 16) {
+      float y[16];
+      tc::ld16(tmem + lane_base + (uint32_t)cb, y);
+      if (valid)
+        for (int o = 0; o < 16 && cb + o < a.Np; ++o) z[c * a.Np + cb + o] = (TV)((double)y[o] * sc);
+    }
     tc::fence_before();
     __syncthreads();
   }
@@ -459,7 +461,8 @@ void LearnedNet::init(int Np_, int64_t ncells_, int nfaces_, int nextra_, const 
   Op = (Np + 15) / 16 * 16;
   require(H % 16 == 0 && H >= 16 && H <= 128, "learned stage: hidden width must be a multiple of 16 in 16..128",
           BSGPU_ERR_UNSUPPORTED);
-  require(Op == 16, "learned stage: at most 16 modes per cell", BSGPU_ERR_UNSUPPORTED);
+  require(Op <= H, "learned stage: the hidden width must be at least the modes per cell (padded to 16)",
+          BSGPU_ERR_UNSUPPORTED);
   require(TcSmem(Fp, H, Op).total <= 200 * 1024, "learned stage: input too wide for one CTA", BSGPU_ERR_UNSUPPORTED);
   err.alloc(1);
   BSGPU_CUDA(cudaMemset(err.p, 0, sizeof(int)));

@@ -980,12 +980,6 @@ struct OrthoT {
   int nslots = 0;
   DBuf<T> W, MW;
   DBuf<T*> d_sol, d_mxx;
-  // FP16 history of the FP32 preconditioner (entries scaled by hscale = sqrt(N)): half the history traffic
-  bool half_hist = false;
-  float hscale = 1.0f;
-  std::vector<DBuf<__half>> HSol, HMxx;
-  DBuf<__half*> h_sol, h_mxx;
-  bool half() const { return sizeof(T) == 4 && half_hist; }
   DBuf<OrthoState> state;
   HistScratch hs;
   double* d_hbeta = nullptr;  // projection coefficients of the recorded form [nslots]
@@ -998,36 +992,19 @@ struct OrthoT {
     if (nslots >= slots) return;
     W.alloc(std::max<int64_t>(N, 1));
     MW.alloc(std::max<int64_t>(N, 1));
-    if (half()) {
-      hscale = (float)std::sqrt((double)std::max<int64_t>(N, 1));
-      while ((int)HSol.size() < slots) {
-        HSol.emplace_back(std::max<int64_t>(N, 1));
-        HMxx.emplace_back(std::max<int64_t>(N, 1));
-      }
-      std::vector<__half*> ps(slots), pm(slots);
-      for (int j = 0; j < slots; ++j) {
-        ps[j] = HSol[j].p;
-        pm[j] = HMxx[j].p;
-      }
-      h_sol.alloc(slots);
-      h_mxx.alloc(slots);
-      BSGPU_CUDA(cudaMemcpy(h_sol.p, ps.data(), slots * sizeof(__half*), cudaMemcpyHostToDevice));
-      BSGPU_CUDA(cudaMemcpy(h_mxx.p, pm.data(), slots * sizeof(__half*), cudaMemcpyHostToDevice));
-    } else {
-      while ((int)Sol.size() < slots) {
-        Sol.emplace_back(std::max<int64_t>(N, 1));
-        Mxx.emplace_back(std::max<int64_t>(N, 1));
-      }
-      std::vector<T*> ps(slots), pm(slots);
-      for (int j = 0; j < slots; ++j) {
-        ps[j] = Sol[j].p;
-        pm[j] = Mxx[j].p;
-      }
-      d_sol.alloc(slots);
-      d_mxx.alloc(slots);
-      BSGPU_CUDA(cudaMemcpy(d_sol.p, ps.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
-      BSGPU_CUDA(cudaMemcpy(d_mxx.p, pm.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
+    while ((int)Sol.size() < slots) {
+      Sol.emplace_back(std::max<int64_t>(N, 1));
+      Mxx.emplace_back(std::max<int64_t>(N, 1));
     }
+    std::vector<T*> ps(slots), pm(slots);
+    for (int j = 0; j < slots; ++j) {
+      ps[j] = Sol[j].p;
+      pm[j] = Mxx[j].p;
+    }
+    d_sol.alloc(slots);
+    d_mxx.alloc(slots);
+    BSGPU_CUDA(cudaMemcpy(d_sol.p, ps.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
+    BSGPU_CUDA(cudaMemcpy(d_mxx.p, pm.data(), slots * sizeof(T*), cudaMemcpyHostToDevice));
     if (!state.p) {
       state.alloc(1);
       BSGPU_CUDA(cudaMemset(state.p, 0, sizeof(OrthoState)));
@@ -1044,15 +1021,6 @@ struct OrthoT {
   // one projection sweep of (W, MW) against the first k history entries; |MW| after it into d_proj[0] and, with
   // `self`, |MW|^2 before it into d_proj[1]
   void cgs_dev(Ctx& c, bool self) {
-    if constexpr (sizeof(T) == 4) {
-      if (half()) {
-        hist_dots(hs, h_mxx.p, &state.p->k, MW.p, N, hscale, d_hbeta, self ? d_proj + 1 : nullptr, c.st);
-        hist_axpy2(h_sol.p, h_mxx.p, &state.p->k, nslots, hscale, d_hbeta, W.p, MW.p, N, c.st);
-        const T* a[1] = {MW.p};
-        dots(c.red, 1, a, a, N, d_proj, 1, c.st);
-        return;
-      }
-    }
     hist_dots(hs, d_mxx.p, &state.p->k, MW.p, N, d_hbeta, self ? d_proj + 1 : nullptr, c.st);
     hist_axpy2(d_sol.p, d_mxx.p, &state.p->k, nslots, d_hbeta, W.p, MW.p, N, c.st);
     const T* a[1] = {MW.p};
@@ -1070,14 +1038,7 @@ struct OrthoT {
     ortho_decide2(state.p, d_proj, c.st);
     c.cond_end();
     ortho_final(state.p, d_proj, c.st);
-    if constexpr (sizeof(T) == 4) {
-      if (half())
-        ortho_store(state.p, W.p, MW.p, h_sol.p, h_mxx.p, nslots, hscale, N, c.d_err, c.st);
-      else
-        ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
-    } else {
-      ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
-    }
+    ortho_store(state.p, W.p, MW.p, d_sol.p, d_mxx.p, nslots, N, c.d_err, c.st);
     ortho_advance(state.p, recalc_period, nslots, c.st);
   }
   void minimize_dev(Ctx& c, T* X, const T* B, const T* Res0, T* Res, const TermParams& tp) {
@@ -2085,7 +2046,6 @@ std::unique_ptr<Solver<T>> build_hlevel(Tree& t, const Matrix* A64, const Matrix
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
-  omg->ortho.half_hist = (t.cfg.fp16_storage & BSGPU_FP16_HISTORY) != 0;
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = cfg.h_sweeps;
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -2165,7 +2125,6 @@ std::unique_ptr<Solver<T>> build_hmg_level(Tree& t, const HmgHierarchy* H, const
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, ht);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
-  omg->ortho.half_hist = (t.cfg.fp16_storage & BSGPU_FP16_HISTORY) != 0;
   omg->trace = c.trace_id(lv + ".OrthoMG");
   omg->sweeps = std::max(1, cfg.h_sweeps);
   omg->post = make_smoother<T>(c, A64, AT, cfg.h_smoother, cfg, lv);
@@ -2230,7 +2189,6 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
   auto omg = std::make_unique<OrthoMGT<T>>(c, AT, lt);
   omg->ortho.cap = std::max(2, t.cfg.ortho_max_krylov > 0 ? t.cfg.ortho_max_krylov : 96);
   omg->ortho.recalc_period = std::max(1, t.cfg.recalc_resi_period);
-  omg->ortho.half_hist = (t.cfg.fp16_storage & BSGPU_FP16_HISTORY) != 0;
   omg->trace = c.trace_id(lv + ".OrthoMG");
   if (level == 0 && t.net && (cfg.learned & BSGPU_LEARNED_PRESMOOTH)) {
     omg->pre = std::make_unique<LearnedPrecondT<T>>(c, t.net.get());

@@ -17,7 +17,7 @@ SOLVER_SOFTPCG, SOLVER_FGMRES_PMG, SOLVER_ORTHOMG, SOLVER_BLOCKJACOBI, SOLVER_SO
 TERM_DEFAULT, TERM_RELATIVE = 0, 1
 COARSE_DENSE, COARSE_PCG, COARSE_AMG, COARSE_HMG = 0, 1, 2, 3
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-FP16_HISTORY, FP16_MATRICES = 1, 2
+FP16_MATRICES = 2
 SMOOTHER_BLOCKJACOBI, SMOOTHER_BLOCKGS, SMOOTHER_SCHWARZ, SMOOTHER_ILU, SMOOTHER_ILU_NATURAL = 0, 1, 2, 3, 4
 SMOOTHER_SCHWARZ_BLOCKS = 5
 LEARNED_OFF, LEARNED_FGMRES, LEARNED_PRESMOOTH, LEARNED_BOTH = 0, 1, 2, 3

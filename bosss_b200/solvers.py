@@ -273,7 +273,6 @@ class PmgConfig(IterativeSolverConfig):
     SchwarzParts: int = 0           # Smoother "schwarz_blocks": number of blocks (0: blocks of 8 cells)
     SchwarzOverlap: int = 1         # ... layers of overlap (0, 1, 2)
     SchwarzOverlapScaling: bool = False
-    HistoryFP16: bool = False       # FP16 OrthoMG histories in the recorded FP32 V-cycle (FGMRESConfig Graph + mixed)
     MatrixFP16: bool = False        # FP16 level matrices in the FP32 V-cycle (FGMRESConfig MixedPrecision)
 
     def _fill(self, c):
@@ -308,7 +307,7 @@ class PmgConfig(IterativeSolverConfig):
         if self.RecalcResiPeriod < 1:
             raise ValueError("RecalcResiPeriod must be at least 1")
         c.recalc_resi_period = self.RecalcResiPeriod
-        c.fp16_storage = (nat.FP16_HISTORY if self.HistoryFP16 else 0) | (nat.FP16_MATRICES if self.MatrixFP16 else 0)
+        c.fp16_storage = nat.FP16_MATRICES if self.MatrixFP16 else 0
         if self.SchwarzOverlap < 0 or self.SchwarzOverlap > 2:
             raise ValueError("SchwarzOverlap must be 0, 1 or 2")
         c.schwarz_parts = self.SchwarzParts

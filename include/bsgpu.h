@@ -142,10 +142,9 @@ enum { BSGPU_COARSE_DENSE = 0, BSGPU_COARSE_PCG = 1, BSGPU_COARSE_AMG = 2,
                                OrthoMG to coarse_tol with h_sweeps block-Jacobi sweeps, h_cycle iterations on the
                                coarser h-levels, dense below dense_limit */ };
 enum { BSGPU_PRECISION_FP64 = 0, BSGPU_PRECISION_MIXED = 1 /* preconditioner in FP32, outer FP64 */ };
-/* FP16 storage inside the FP32 preconditioner: OrthoMG histories (with cfg.graph; scaled by sqrt(n), which keeps
- * a normalised vector's entries in FP16's normal range) and the level matrices (uniform blocks of 4, 10 or 20;
- * not with the Gauss-Seidel smoother) */
-enum { BSGPU_FP16_HISTORY = 1, BSGPU_FP16_MATRICES = 2 };
+/* FP16 storage inside the FP32 preconditioner: the level matrices (uniform blocks of 4, 10 or 20; not with the
+ * Gauss-Seidel smoother).  Bit 1 is reserved (FP16 OrthoMG histories lost the minimisation's consistency). */
+enum { BSGPU_FP16_MATRICES = 2 };
 /* post-smoother of the OrthoMG levels: BlockJacobi (BlockJacobi.cs:35; NoOfIterations = bj_iters), symmetric
  * multicolour block Gauss-Seidel (max(1, bj_iters) symmetric sweeps; uniform blocks of 4, 6, 10 or 20), or
  * restricted additive Schwarz with one overlapping block per cell (Schwarz.cs:56; bj_iters + 1 updates; blocks

@@ -162,3 +162,24 @@ def test_training_collects_requested_pairs(cuda):
     assert slv.Converged
     slv.Dispose()
     op.Dispose()
+
+
+def test_learned_forward_twenty_modes(cuda):
+    """Np = 20 (p = 3): the output layer has two 16-column halves in tensor memory; the forward pass against the
+    BF16-emulating PyTorch evaluation."""
+    import torch
+    s = A.poisson_3d(5, 3, seed=2)
+    op = MultigridOperator(BlockMsrMatrix.from_system(s))
+    nbr = s.grid.face_neighbours()
+    op.SetCellGraph(nbr)
+    slv = FGMRESConfig(Learned="fgmres", Preconditioners=[PmgConfig(DegreeHierarchy=(20, 10, 4))]).CreateInstance(op)
+    info = slv.LearnedInfo()
+    assert info["Np"] == 20 and info["Op"] == 32 and info["F"] == 140
+    W = slv.LearnedWeights()
+    r = np.random.default_rng(8).standard_normal(s.N)
+    z = slv.ApplyLearned(r)
+    emul = _forward(r, nbr, np.zeros((s.nb, 0), np.float32), W, info, torch.float32, True).double().numpy()
+    e = np.linalg.norm(z - emul) / np.linalg.norm(emul)
+    assert e <= 2e-3, e
+    slv.Dispose()
+    op.Dispose()
