@@ -59,14 +59,20 @@ def parse():
     ap.add_argument("--concurrency", type=int, default=16, help="xdgbatch: problems solved at once")
     ap.add_argument("--learned", default="off", help="varcoef96/xdgbatch: learned stage mode")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
-                    help="fast form without the graph-recorded V-cycle")
+                    help="fast form without graph recording")
+    ap.add_argument("--graph-mode", default="vcycle", choices=["vcycle", "solve"],
+                    help="fast form: record the V-cycle (one graph launch per preconditioner application) or the whole "
+                         "FlexGMRES solve (one launch per solve; xdgbatch: one launch per wave)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="fast form without the launch-shape autotuner")
     ap.add_argument("--no-learned-variant", dest="learned_variant", action="store_false",
                     help="default workload: skip the learned-stage variant")
     ap.add_argument("--fp16", default="none", choices=["none", "matrices"],
                     help="FP16 level matrices inside the fast form's FP32 preconditioner (weaker preconditioner)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.graph:
+        args.graph = args.graph_mode
+    return args
 
 
 def levels_for(p: int):
@@ -666,7 +672,8 @@ def run_single_system(args, s, workload, prepare=None):
                    "fast": ("FP32 block-Jacobi" if fast_name == "mixed_bj" else "FP32 Schwarz")
                            + " p-MG inside FP64 FlexGMRES" + ("" if args.learned == "off" else
                                                               f" + learned stage ({args.learned})")
-                           + (", V-cycle as one CUDA graph" if args.graph else "")
+                           + ({"vcycle": ", V-cycle as one CUDA graph", "solve": ", whole solve as one CUDA graph"}
+                              .get(args.graph, ""))
                            + (", autotuned launch shapes" if args.autotune else "")
                            + (f", FP16 storage ({args.fp16})" if args.fp16 != "none" else ""),
                    "plain": "FP64 block-Jacobi p-MG inside FP64 FlexGMRES"},
@@ -802,7 +809,8 @@ def run_xdg_batch(args):
     launches0 = nat.launch_count()
     out = BatchSolver(lambda op: {"fast": _fgmres(op, PMG_SCHWARZ, True, graph=args.graph, tune=args.autotune),
                                   "plain_fp64": _fgmres(op, PMG_BJ, False)},
-                      concurrency=args.concurrency).run(_bounded_imap(pool, _gen_xdg, mine, 2 * args.concurrency))
+                      concurrency=args.concurrency, one_graph=["fast"] if args.graph == "solve" else []
+                      ).run(_bounded_imap(pool, _gen_xdg, mine, 2 * args.concurrency))
     wall = time.perf_counter() - t0
     launches = nat.launch_count() - launches0
     pool.close()
@@ -817,7 +825,9 @@ def run_xdg_batch(args):
         "ms_per_step": agg["seconds"] * 1e3, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f64 (outer) / f32 (preconditioner)", "data": "synthetic (seeded problems)",
         "config": {"workload": f"{args.batch} {XDGBATCH}", "concurrency": args.concurrency, "tol": TOL,
-                   "parallelism": f"replicas x{ws} (problems sharded)", "host_generation_procs": procs},
+                   "parallelism": f"replicas x{ws} (problems sharded)", "host_generation_procs": procs,
+                   "fast_graph": args.graph, "fast_wave": "one graph launch" if args.graph == "solve" else
+                   "host threads, one stream per problem"},
         "fast": fast, "plain_fp64": plain, "plain_fp64_dof_per_s": agg_plain["per_s"],
         "speedup_vs_plain_fp64": agg["per_s"] / agg_plain["per_s"], "wall_s_incl_generation": wall,
         "gpu_launches": launches,

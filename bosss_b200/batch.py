@@ -66,13 +66,16 @@ class BatchSolver:
     """
 
     def __init__(self, make_solver: Callable, concurrency: int = 8, prepare: Optional[Callable] = None,
-                 device: str = "cuda"):
+                 device: str = "cuda", one_graph: Iterable[str] = ()):
         if concurrency < 1:
             raise ValueError("concurrency must be at least 1")
         self.make_solver = make_solver
         self.concurrency = concurrency
         self.prepare = prepare
         self.device = device
+        # configuration names whose waves run as one CUDA graph (GpuBatch; their solvers are created with
+        # FGMRESConfig(Graph="solve")); the other configurations run from host threads
+        self.one_graph = set(one_graph)
 
     def _setup(self, system):
         import torch
@@ -89,9 +92,24 @@ class BatchSolver:
         torch.cuda.synchronize()
         return dict(M=M, op=op, slv=slvs, B=B, X=X, setup_s=time.perf_counter() - t0, dof=int(system.N))
 
-    def run(self, systems: Iterable, on_result: Optional[Callable] = None) -> Dict[str, BatchSummary]:
-        """Returns one summary per configuration name ("" for a single solver)."""
+    @staticmethod
+    def _collect(name, wave, times, results, on_result):
         import torch
+        for i, w in wave:
+            r = w["B"].clone()
+            w["M"].SpMV(-1.0, w["X"][name], 1.0, r)
+            rel = (torch.linalg.norm(r) / torch.linalg.norm(w["B"])).item()
+            slv = w["slv"][name]
+            res = BatchResult(index=i, dof=w["dof"], setup_s=w["setup_s"], solve_s=times[i],
+                              iterations=slv.ThisLevelIterations, converged=slv.Converged, relres=rel)
+            results.setdefault(name, []).append(res)
+            if on_result is not None:
+                on_result(name, res, w)
+
+    def run(self, systems: Iterable, on_result: Optional[Callable] = None) -> Dict[str, BatchSummary]:
+        """Returns one summary per configuration name ("" for a single solver).  Per-system solve_s: the host wall
+        time of its Solve call (threads), or the device time from the wave's graph launch to the end of its branch
+        (one-graph waves)."""
         results: Dict[str, List[BatchResult]] = {}
         solve_wall: Dict[str, float] = {}
         setup_wall = 0.0
@@ -111,6 +129,22 @@ class BatchSolver:
             for name in wave[0][1]["slv"]:
                 times = {}
                 errors = []
+                if name in self.one_graph:
+                    from .solvers import GpuBatch
+                    t1 = time.perf_counter()
+                    gb = GpuBatch([w["slv"][name] for _, w in wave])  # records the wave's graph (set-up)
+                    setup_wall += time.perf_counter() - t1
+                    a = time.perf_counter()
+                    try:
+                        gb.Solve([w["X"][name] for _, w in wave], [w["B"] for _, w in wave])
+                    finally:
+                        lat = gb.Latencies()
+                        gb.Dispose()
+                    solve_wall[name] = solve_wall.get(name, 0.0) + time.perf_counter() - a
+                    for (i, _), sec in zip(wave, lat):
+                        times[i] = sec
+                    self._collect(name, wave, times, results, on_result)
+                    continue
 
                 def work(i, w, key):
                     try:
@@ -129,16 +163,7 @@ class BatchSolver:
                 solve_wall[name] = solve_wall.get(name, 0.0) + time.perf_counter() - a
                 if errors:
                     raise errors[0]
-                for i, w in wave:
-                    r = w["B"].clone()
-                    w["M"].SpMV(-1.0, w["X"][name], 1.0, r)
-                    rel = (torch.linalg.norm(r) / torch.linalg.norm(w["B"])).item()
-                    slv = w["slv"][name]
-                    res = BatchResult(index=i, dof=w["dof"], setup_s=w["setup_s"], solve_s=times[i],
-                                      iterations=slv.ThisLevelIterations, converged=slv.Converged, relres=rel)
-                    results.setdefault(name, []).append(res)
-                    if on_result is not None:
-                        on_result(name, res, w)
+                self._collect(name, wave, times, results, on_result)
             for i, w in wave:
                 for slv in w["slv"].values():
                     slv.Dispose()

@@ -1,6 +1,7 @@
 // extern "C" boundary of the library (declarations and reference citations in include/bsgpu.h).
 #include <atomic>
 #include <cstring>
+#include <exception>
 #include <memory>
 
 #include "solvers.cuh"
@@ -31,6 +32,39 @@ struct bsgpu_solver_s {
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   std::vector<double> history;
   double* lscal = nullptr;  // device scalars of the learned-stage entry points
+  // cfg.graph == 2: the whole solve (change of basis, FlexGMRES with its V-cycle, back-transform) recorded once on
+  // the staging vectors X, B and replayed by one graph launch
+  cudaGraphExec_t rec_exec = nullptr;
+  long long rec_top = 0;  // kernels at the top level of the recording
+  int rec_key = -1;
+  ~bsgpu_solver_s() {
+    if (rec_exec) cudaGraphExecDestroy(rec_exec);
+  }
+};
+
+// Many handles recorded as one CUDA graph: every handle's recorded solve is one branch of the graph, all branches
+// run concurrently from one launch.
+struct bsgpu_batch_s {
+  std::vector<bsgpu_solver_s*> s;
+  std::vector<int> keys;
+  cudaStream_t st = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long top = 0;
+  cudaEvent_t start = nullptr;
+  std::vector<cudaEvent_t> done;  // recorded at the end of every branch (external event nodes)
+  bsgpu::DBuf<const double*> src;
+  bsgpu::DBuf<double*> dst;
+  bsgpu::DBuf<int64_t> len;
+  const double** h_src = nullptr;  // pinned staging of the copy tables
+  double** h_dst = nullptr;
+  ~bsgpu_batch_s() {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (cudaEvent_t e : done) cudaEventDestroy(e);
+    if (start) cudaEventDestroy(start);
+    if (st) cudaStreamDestroy(st);
+    if (h_src) cudaFreeHost(h_src);
+    if (h_dst) cudaFreeHost(h_dst);
+  }
 };
 
 namespace bsgpu {
@@ -83,10 +117,79 @@ void from_transformed(bsgpu_mgop_s* op, const double* Xt, double* X, cudaStream_
   block_gemv(op->L.p, A.doff.p, A.len.p, A.i0.p, A.row2blk.p, A.uniform ? A.Np : 0, true, Xt, X, A.N, st);
 }
 
+// The recorded solve of a handle: staging vectors X, B -> transformed basis, FlexGMRES, back into X.
+void record_branch(bsgpu_solver_s* s, RecordedSolve* r) {
+  Ctx& c = *s->tree->ctx;
+  to_transformed(s->op, s->X.p, s->B.p, s->Xt.p, s->Bt.p, c.st);
+  r->record(c, s->Xt.p, s->Bt.p);
+  from_transformed(s->op, s->Xt.p, s->X.p, c.st);
+}
+
+// (Re)records the handle's whole solve when there is none or the learned stage was switched since.
+void ensure_recorded(bsgpu_solver_s* s) {
+  RecordedSolve* r = recorded_form(*s->tree);
+  if (!r || (s->rec_exec && r->key() == s->rec_key)) return;
+  if (s->rec_exec) {
+    cudaGraphExecDestroy(s->rec_exec);
+    s->rec_exec = nullptr;
+  }
+  Ctx& c = *s->tree->ctx;
+  r->prepare(c);
+  c.capture_begin();
+  cudaGraph_t g = nullptr;
+  try {
+    record_branch(s, r);
+  } catch (...) {
+    c.capture_abort();
+    cudaStreamEndCapture(c.st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  s->rec_top = c.capture_end(&g);
+  const cudaError_t e = cudaGraphInstantiate(&s->rec_exec, g, 0);
+  cudaGraphDestroy(g);
+  BSGPU_CUDA(e);
+  s->rec_key = r->key();
+}
+
+void fill_stats(bsgpu_solver_s* s, bsgpu_solve_stats* stats, double seconds) {
+  Tree& t = *s->tree;
+  s->history = t.top->history;
+  if (!stats) return;
+  stats->iterations = t.top->this_level_iterations;
+  stats->nested = t.top->nested();
+  stats->converged = t.top->converged ? 1 : 0;
+  stats->n_history = (int32_t)s->history.size();
+  stats->res0 = s->history.empty() ? 0.0 : s->history.front();
+  stats->res = s->history.empty() ? 0.0 : s->history.back();
+  stats->seconds = seconds;
+}
+
 void solve_device(bsgpu_solver_s* s, double* dX, const double* dB, bsgpu_solve_stats* stats) {
   Tree& t = *s->tree;
   Ctx& c = *t.ctx;
   const int64_t N = s->op->A->N;
+  RecordedSolve* rec = recorded_form(t);
+  if (rec && !c.tracing && !t.collect) {
+    ensure_recorded(s);
+    BSGPU_CUDA(cudaEventRecord(s->e0, c.st));
+    if (N && dX != s->X.p) BSGPU_CUDA(cudaMemcpyAsync(s->X.p, dX, N * 8, cudaMemcpyDeviceToDevice, c.st));
+    if (N && dB != s->B.p) BSGPU_CUDA(cudaMemcpyAsync(s->B.p, dB, N * 8, cudaMemcpyDeviceToDevice, c.st));
+    BSGPU_CUDA(cudaGraphLaunch(s->rec_exec, c.st));
+    add_launches(s->rec_top);
+    c.graph_ran = true;
+    if (N && dX != s->X.p) BSGPU_CUDA(cudaMemcpyAsync(dX, s->X.p, N * 8, cudaMemcpyDeviceToDevice, c.st));
+    BSGPU_CUDA(cudaEventRecord(s->e1, c.st));
+    rec->queue_result(c, c.st);
+    BSGPU_CUDA(cudaStreamSynchronize(c.st));
+    rec->take_result(c);
+    c.flush_graph_counts();  // raises an error the device recorded
+    if (t.net) learned_check(*t.net, c.st);
+    float ms = 0;
+    BSGPU_CUDA(cudaEventElapsedTime(&ms, s->e0, s->e1));
+    fill_stats(s, stats, ms * 1e-3);
+    return;
+  }
   BSGPU_CUDA(cudaEventRecord(s->e0, c.st));
   to_transformed(s->op, dX, dB, s->Xt.p, s->Bt.p, c.st);
   t.top->this_level_iterations = 0;
@@ -98,16 +201,7 @@ void solve_device(bsgpu_solver_s* s, double* dX, const double* dB, bsgpu_solve_s
   if (t.net) learned_check(*t.net, c.st);
   float ms = 0;
   BSGPU_CUDA(cudaEventElapsedTime(&ms, s->e0, s->e1));
-  s->history = t.top->history;
-  if (stats) {
-    stats->iterations = t.top->this_level_iterations;
-    stats->nested = t.top->nested();
-    stats->converged = t.top->converged ? 1 : 0;
-    stats->n_history = (int32_t)s->history.size();
-    stats->res0 = s->history.empty() ? 0.0 : s->history.front();
-    stats->res = s->history.empty() ? 0.0 : s->history.back();
-    stats->seconds = ms * 1e-3;
-  }
+  fill_stats(s, stats, ms * 1e-3);
   (void)N;
 }
 
@@ -393,8 +487,134 @@ BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgp
     h->X.alloc(N); h->B.alloc(N); h->Xt.alloc(N); h->Bt.alloc(N);
     BSGPU_CUDA(cudaEventCreate(&h->e0));
     BSGPU_CUDA(cudaEventCreate(&h->e1));
+    ensure_recorded(h.get());  // cfg.graph == 2: the whole solve is recorded at set-up
     *s = h.release();
   });
+}
+
+BSGPU_API int bsgpu_batch_create(bsgpu_batch_t* b, const bsgpu_solver_t* solvers, int32_t n) {
+  return guarded([&] {
+    require(b && solvers && n >= 1, "null argument or empty batch");
+    auto h = std::make_unique<bsgpu_batch_s>();
+    for (int32_t i = 0; i < n; ++i) {
+      bsgpu_solver_s* s = solvers[i];
+      require(s != nullptr, "null solver handle in the batch");
+      for (int32_t q = 0; q < i; ++q) require(solvers[q] != s, "a solver handle appears twice in the batch");
+      RecordedSolve* r = recorded_form(*s->tree);
+      require(r != nullptr, "batch members must be FlexGMRES solvers created with graph = 2", BSGPU_ERR_UNSUPPORTED);
+      r->prepare(*s->tree->ctx);
+      BSGPU_CUDA(cudaStreamSynchronize(s->tree->ctx->st));
+      h->s.push_back(s);
+      h->keys.push_back(r->key());
+    }
+    BSGPU_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    BSGPU_CUDA(cudaEventCreate(&h->start));
+    h->done.assign(n, nullptr);
+    for (auto& e : h->done) BSGPU_CUDA(cudaEventCreate(&e));
+    h->src.alloc(3 * n);  // copy tables: right-hand sides in, initial guesses in, solutions out
+    h->dst.alloc(3 * n);
+    h->len.alloc(n);
+    BSGPU_CUDA(cudaMallocHost(&h->h_src, 3 * n * sizeof(double*)));
+    BSGPU_CUDA(cudaMallocHost(&h->h_dst, 3 * n * sizeof(double*)));
+    std::vector<int64_t> lens(n);
+    for (int32_t i = 0; i < n; ++i) lens[i] = h->s[i]->op->A->N;
+    BSGPU_CUDA(cudaMemcpy(h->len.p, lens.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice));
+    cudaEvent_t fork = nullptr, join = nullptr;
+    BSGPU_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    BSGPU_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    cudaGraph_t g = nullptr;
+    BSGPU_CUDA(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed));
+    int32_t i = 0;
+    try {
+      BSGPU_CUDA(cudaEventRecord(fork, h->st));
+      for (; i < n; ++i) {
+        Ctx& c = *h->s[i]->tree->ctx;
+        BSGPU_CUDA(cudaStreamWaitEvent(c.st, fork, 0));
+        c.capture_join();
+        record_branch(h->s[i], recorded_form(*h->s[i]->tree));
+        h->top += c.capture_leave();
+        BSGPU_CUDA(cudaEventRecordWithFlags(h->done[i], c.st, cudaEventRecordExternal));
+        BSGPU_CUDA(cudaEventRecord(join, c.st));
+        BSGPU_CUDA(cudaStreamWaitEvent(h->st, join, 0));
+      }
+    } catch (...) {
+      if (i < n) {
+        Ctx& c = *h->s[i]->tree->ctx;
+        c.capture_abort();
+        cudaEventRecord(join, c.st);
+        cudaStreamWaitEvent(h->st, join, 0);
+      }
+      cudaStreamEndCapture(h->st, &g);
+      if (g) cudaGraphDestroy(g);
+      cudaEventDestroy(fork);
+      cudaEventDestroy(join);
+      throw;
+    }
+    BSGPU_CUDA(cudaStreamEndCapture(h->st, &g));
+    cudaEventDestroy(fork);
+    cudaEventDestroy(join);
+    const cudaError_t e = cudaGraphInstantiate(&h->exec, g, 0);
+    cudaGraphDestroy(g);
+    BSGPU_CUDA(e);
+    *b = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_batch_solve_device(bsgpu_batch_t b, double* const* X, const double* const* B,
+                                       bsgpu_solve_stats* stats) {
+  return guarded([&] {
+    require(b && X && B, "null argument");
+    const int n = (int)b->s.size();
+    for (int i = 0; i < n; ++i) {
+      require(X[i] && B[i], "null vector in the batch");
+      require(recorded_form(*b->s[i]->tree)->key() == b->keys[i],
+              "a batch member's learned stage was switched after the batch was recorded; create the batch again");
+    }
+    cudaStream_t st = b->st;
+    // staging: B_i -> handle i's B, X_i -> handle i's X (initial guess) before the graph, handle i's X -> X_i after
+    for (int i = 0; i < n; ++i) {
+      b->h_src[i] = B[i];
+      b->h_dst[i] = b->s[i]->B.p;
+      b->h_src[n + i] = X[i];
+      b->h_dst[n + i] = b->s[i]->X.p;
+      b->h_src[2 * n + i] = b->s[i]->X.p;
+      b->h_dst[2 * n + i] = X[i];
+    }
+    // ordered after the caller's work on the legacy default stream, as bsgpu_solver_solve_device
+    BSGPU_CUDA(cudaEventRecord(b->start, cudaStreamLegacy));
+    BSGPU_CUDA(cudaStreamWaitEvent(st, b->start, 0));
+    BSGPU_CUDA(cudaMemcpyAsync(b->src.p, b->h_src, 3 * n * sizeof(double*), cudaMemcpyHostToDevice, st));
+    BSGPU_CUDA(cudaMemcpyAsync(b->dst.p, b->h_dst, 3 * n * sizeof(double*), cudaMemcpyHostToDevice, st));
+    batch_copy(b->src.p, b->dst.p, b->len.p, n, st);
+    batch_copy(b->src.p + n, b->dst.p + n, b->len.p, n, st);
+    BSGPU_CUDA(cudaEventRecord(b->start, st));
+    BSGPU_CUDA(cudaGraphLaunch(b->exec, st));
+    add_launches(b->top);
+    batch_copy(b->src.p + 2 * n, b->dst.p + 2 * n, b->len.p, n, st);
+    for (int i = 0; i < n; ++i) recorded_form(*b->s[i]->tree)->queue_result(*b->s[i]->tree->ctx, st);
+    BSGPU_CUDA(cudaStreamSynchronize(st));
+    // results of every member first, then the first error any of them recorded
+    std::exception_ptr first;
+    for (int i = 0; i < n; ++i) {
+      bsgpu_solver_s* s = b->s[i];
+      Ctx& c = *s->tree->ctx;
+      recorded_form(*s->tree)->take_result(c);
+      c.graph_ran = true;
+      float ms = 0;
+      BSGPU_CUDA(cudaEventElapsedTime(&ms, b->start, b->done[i]));
+      fill_stats(s, stats ? stats + i : nullptr, ms * 1e-3);
+      try {
+        c.flush_graph_counts();
+      } catch (...) {
+        if (!first) first = std::current_exception();
+      }
+    }
+    if (first) std::rethrow_exception(first);
+  });
+}
+
+BSGPU_API int bsgpu_batch_destroy(bsgpu_batch_t b) {
+  return guarded([&] { delete b; });
 }
 
 BSGPU_API int bsgpu_solver_destroy(bsgpu_solver_t s) {

@@ -28,6 +28,36 @@ __device__ bool term_continue(const TermParams& t, int iter, double R0, double R
   return true;
 }
 
+// Term::operator() (solvers.cu) on the device: returns "continue", writes "converged".
+__device__ bool term_eval(const TermParams& t, int iter, double R0, double R, bool* conv) {
+  const double eps = 2.2204460492503131e-16 * 1000;
+  *conv = false;
+  if (t.mode == 2) {
+    *conv = true;
+    return iter <= t.max_iter;
+  }
+  if (t.mode == 3) {
+    if (iter <= 1) return true;
+    if (R < R0 * t.reduction) {
+      *conv = true;
+      return false;
+    }
+    return iter <= t.max_iter;
+  }
+  if (iter <= t.min_iter) return true;
+  const bool ok = (t.mode == 0) ? (R < R0 * t.tol + t.tol) : (R < R0 * t.tol);
+  if (ok) {
+    *conv = true;
+    return false;
+  }
+  if (iter > t.max_iter) return false;
+  if (R0 < eps || R < eps) {
+    *conv = true;
+    return false;
+  }
+  return true;
+}
+
 __global__ void cond_set_kernel(cudaGraphConditionalHandle h, const int* a, const int* not_b, const int* k, int cap,
                                 unsigned int* exec) {
   bool v = true;
@@ -313,6 +343,195 @@ __global__ void copy_if_kernel(const T* __restrict__ x, T* __restrict__ y, int64
     y[i] = x[i];
 }
 
+// ---- recorded FlexGMRES (FlexGMRES.cs:144-277) ----
+
+__global__ void fg_begin_kernel(FgState* s, int nn_active, int has2) {
+  s->j = 0;
+  s->k1 = 1;
+  s->kk = 0;
+  s->iter = 0;
+  s->outer = 0;
+  s->inner = 0;
+  s->use2 = 0;
+  s->nn_active = nn_active;
+  s->turn = 0;
+  s->converged = 0;
+  s->nhist = 0;
+  s->stalled = 0;
+  s->started = 0;
+  s->has2 = has2;
+  s->zero = 0;
+  s->r0 = 0.0;
+  s->est = 0.0;
+  s->g_before = 0.0;
+  s->inv = 0.0;
+}
+
+// The residual test at the top of every restart cycle (FlexGMRES.cs:168-182).
+__global__ void fg_restart_kernel(FgState* s, FgArrays a, const double* rn, TermParams tp, int* err) {
+  const double r = *rn;
+  s->inner = 0;
+  if (*err != 0) {  // an error raised inside the preconditioner ends the solve (the host raises it)
+    s->outer = 0;
+    return;
+  }
+  if (!isfinite(r)) {
+    atomicOr(err, kDevErrKrylovNaN);
+    s->outer = 0;
+    return;
+  }
+  if (!s->started) {
+    s->r0 = r;
+    s->started = 1;
+  }
+  if (s->nhist < a.hcap) a.hist[s->nhist++] = r;
+  bool conv = false;
+  const bool cont = term_eval(tp, s->iter, s->r0, r, &conv) && s->iter < kMaxRecordedIterations;
+  if (!cont) {
+    s->converged = conv ? 1 : 0;
+    s->outer = 0;
+    return;
+  }
+  s->outer = 1;
+  s->inner = 1;
+  s->inv = r > 0.0 ? 1.0 / r : 0.0;
+  a.g[0] = r;
+  for (int i = 1; i <= a.m; ++i) a.g[i] = 0.0;
+  s->j = 0;
+  s->k1 = 1;
+}
+
+// Round-robin of the preconditioners (FlexGMRES.cs:196-199): every second step uses the second one while it is
+// active.
+__global__ void fg_step_begin_kernel(FgState* s, FgArrays a) {
+  const int j = s->j;
+  s->k1 = j + 1;
+  s->use2 = (s->has2 && s->nn_active && (s->turn % 2 == 1)) ? 1 : 0;
+  s->turn += 1;
+  s->g_before = fabs(a.g[j]);
+}
+
+__global__ void fg_step_end_kernel(FgState* s, FgArrays a, const double* h1, const double* h2, const double* wn_p,
+                                   TermParams tp, double stall, int* err) {
+  const int j = s->j, m = a.m;
+  const double wn = *wn_p;
+  s->iter += 1;
+  if (!isfinite(wn)) {
+    atomicOr(err, kDevErrKrylovNaN);
+    s->inner = 0;
+    s->outer = 0;
+    s->kk = 0;
+    s->inv = 0.0;
+    return;
+  }
+  double* H = a.H;
+  for (int i = 0; i <= j; ++i) H[i * m + j] = h1[i] + h2[i];
+  H[(j + 1) * m + j] = wn;
+  s->inv = wn > 0.0 ? 1.0 / wn : 0.0;
+  for (int i = 0; i < j; ++i) {
+    const double a0 = H[i * m + j], b0 = H[(i + 1) * m + j];
+    H[i * m + j] = a.cs[i] * a0 + a.sn[i] * b0;
+    H[(i + 1) * m + j] = -a.sn[i] * a0 + a.cs[i] * b0;
+  }
+  const double a0 = H[j * m + j], b0 = H[(j + 1) * m + j];
+  const double den = hypot(a0, b0);
+  a.cs[j] = a0 / den;
+  a.sn[j] = b0 / den;
+  H[j * m + j] = den;
+  H[(j + 1) * m + j] = 0.0;
+  a.g[j + 1] = -a.sn[j] * a.g[j];
+  a.g[j] = a.cs[j] * a.g[j];
+  const double est = fabs(a.g[j + 1]);
+  s->est = est;
+  if (s->nhist < a.hcap) a.hist[s->nhist++] = est;
+  if (s->use2 && est > stall * s->g_before) {
+    s->nn_active = 0;  // the second preconditioner stalls: the first one for the rest of this solve
+    s->stalled = 1;
+  }
+  bool conv = false;
+  const bool cont = term_eval(tp, s->iter, s->r0, est, &conv);
+  const bool stop = !cont || conv || wn == 0.0 || s->iter >= kMaxRecordedIterations || *err != 0;
+  s->j = j + 1;
+  s->kk = j + 1;
+  s->inner = (!stop && j + 1 < m) ? 1 : 0;
+}
+
+__global__ void fg_backsub_kernel(FgState* s, FgArrays a) {
+  const int kk = s->kk, m = a.m;
+  for (int i = kk - 1; i >= 0; --i) {
+    double v = a.g[i];
+    for (int q = i + 1; q < kk; ++q) v += a.H[i * m + q] * a.ny[q];  // ny = -y
+    a.ny[i] = -(v / a.H[i * m + i]);
+  }
+}
+
+__global__ void slot_load_kernel(const double* const* __restrict__ tab, const int* __restrict__ idx,
+                                 double* __restrict__ out, int64_t n) {
+  const double* x = tab[idx ? *idx : 0];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = x[i];
+}
+
+__global__ void slot_store_kernel(const double* __restrict__ x, const double* __restrict__ scale,
+                                  double* const* __restrict__ tab, const int* __restrict__ idx, int nslots, int64_t n,
+                                  int* __restrict__ err) {
+  const int k = idx ? *idx : 0;
+  if (k < 0 || k >= nslots) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(err, kDevErrSlots);
+    return;
+  }
+  const double f = scale ? *scale : 1.0;
+  double* y = tab[k];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i] * f;
+}
+
+// y -= sum_{j<k} beta[j] x[j] (FP64, one vector)
+__global__ void __launch_bounds__(kThreads) hist_axpy1_kernel(const double* const* __restrict__ x,
+                                                              const int* __restrict__ kp, int kmax,
+                                                              const double* __restrict__ beta,
+                                                              double* __restrict__ y, int64_t n) {
+  const int k = min(*kp, min(kmax, kHistMax));
+  if (k <= 0) return;
+  __shared__ const double* p[kHistMax];
+  __shared__ double c[kHistMax];
+  for (int j = threadIdx.x; j < k; j += kThreads) {
+    p[j] = x[j];
+    c[j] = beta[j];
+  }
+  __syncthreads();
+  const int64_t nv = n / 2;
+  const int64_t stride = (int64_t)gridDim.x * kThreads;
+  for (int64_t i = (int64_t)blockIdx.x * kThreads + threadIdx.x; i < nv; i += stride) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double2 u = __ldcs(reinterpret_cast<const double2*>(p[j]) + i);
+      a0 = fma(c[j], u.x, a0);
+      a1 = fma(c[j], u.y, a1);
+    }
+    double2 o = reinterpret_cast<double2*>(y)[i];
+    o.x -= a0;
+    o.y -= a1;
+    reinterpret_cast<double2*>(y)[i] = o;
+  }
+  for (int64_t i = nv * 2 + (int64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += stride) {
+    double a0 = 0.0;
+    for (int j = 0; j < k; ++j) a0 = fma(c[j], p[j][i], a0);
+    y[i] -= a0;
+  }
+}
+
+__global__ void batch_copy_kernel(const double* const* __restrict__ src, double* const* __restrict__ dst,
+                                  const int64_t* __restrict__ len, int count) {
+  for (int b = blockIdx.y; b < count; b += gridDim.y) {
+    const double* x = src[b];
+    double* y = dst[b];
+    const int64_t n = len[b];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      y[i] = x[i];
+  }
+}
+
 int grid_for(int64_t n_work) {
   return (int)std::max<int64_t>(1, std::min<int64_t>((n_work + kThreads - 1) / kThreads, (int64_t)num_sms() * 2));
 }
@@ -439,6 +658,52 @@ void copy_if(const double* x, double* y, int64_t n, const int* flag, cudaStream_
 }
 void copy_if(const float* x, float* y, int64_t n, const int* flag, cudaStream_t st) {
   copy_if_impl<float>(x, y, n, flag, st);
+}
+
+
+void hist_axpy1(const double* const* x, const int* k, int kmax, const double* beta, double* y, int64_t n,
+                cudaStream_t st) {
+  require((reinterpret_cast<uintptr_t>(y) & 15) == 0, "history multi-axpy: unaligned vector");
+  require(kmax >= 1 && kmax <= kHistMax, "history multi-axpy: 1 <= slots <= 128");
+  hist_axpy1_kernel<<<grid_for(std::max<int64_t>(n / 2, 1)) * 2, kThreads, 0, st>>>(x, k, kmax, beta, y, n);
+  BSGPU_CHECK_LAUNCH();
+}
+
+void fg_begin(FgState* s, int nn_active, int has2, cudaStream_t st) {
+  fg_begin_kernel<<<1, 1, 0, st>>>(s, nn_active, has2);
+  BSGPU_CHECK_LAUNCH();
+}
+void fg_restart(FgState* s, FgArrays a, const double* rn, TermParams tp, int* err, cudaStream_t st) {
+  fg_restart_kernel<<<1, 1, 0, st>>>(s, a, rn, tp, err);
+  BSGPU_CHECK_LAUNCH();
+}
+void fg_step_begin(FgState* s, FgArrays a, cudaStream_t st) {
+  fg_step_begin_kernel<<<1, 1, 0, st>>>(s, a);
+  BSGPU_CHECK_LAUNCH();
+}
+void fg_step_end(FgState* s, FgArrays a, const double* h1, const double* h2, const double* wn, TermParams tp,
+                 double stall, int* err, cudaStream_t st) {
+  fg_step_end_kernel<<<1, 1, 0, st>>>(s, a, h1, h2, wn, tp, stall, err);
+  BSGPU_CHECK_LAUNCH();
+}
+void fg_backsub(FgState* s, FgArrays a, cudaStream_t st) {
+  fg_backsub_kernel<<<1, 1, 0, st>>>(s, a);
+  BSGPU_CHECK_LAUNCH();
+}
+void slot_load(const double* const* tab, const int* idx, double* out, int64_t n, cudaStream_t st) {
+  slot_load_kernel<<<grid_for(n) * 4, kThreads, 0, st>>>(tab, idx, out, n);
+  BSGPU_CHECK_LAUNCH();
+}
+void slot_store(const double* x, const double* scale, double* const* tab, const int* idx, int nslots, int64_t n,
+                int* err, cudaStream_t st) {
+  slot_store_kernel<<<grid_for(n) * 4, kThreads, 0, st>>>(x, scale, tab, idx, nslots, n, err);
+  BSGPU_CHECK_LAUNCH();
+}
+
+void batch_copy(const double* const* src, double* const* dst, const int64_t* n, int count, cudaStream_t st) {
+  if (count <= 0) return;
+  batch_copy_kernel<<<dim3(32, std::min(count, 65535)), kThreads, 0, st>>>(src, dst, n, count);
+  BSGPU_CHECK_LAUNCH();
 }
 
 }  // namespace bsgpu

@@ -14,7 +14,7 @@
 namespace bsgpu {
 
 // Bits of the device error word of a captured solve (read by the host after the graph).
-enum { kDevErrNaN = 1, kDevErrResidualIncrease = 2, kDevErrSlots = 4 };
+enum { kDevErrNaN = 1, kDevErrResidualIncrease = 2, kDevErrSlots = 4, kDevErrKrylovNaN = 8 };
 
 // Device state of one OrthonormalizationMultigrid level (CoreOrthonormalizationProcedure + loop).
 struct OrthoState {
@@ -88,6 +88,65 @@ void level_begin(OrthoState* s, const double* r0_in, TermParams tp, cudaStream_t
 void iter_begin(OrthoState* s, int cap, cudaStream_t st);
 // end of an iteration: iterations += active, iter += 1, active = active && term(iter, r0, rn)
 void iter_end(OrthoState* s, TermParams tp, cudaStream_t st);
+// y -= sum_{j<*k} beta[j] x[j]; one launch (the single-vector form of hist_axpy2)
+void hist_axpy1(const double* const* x, const int* k, int kmax, const double* beta, double* y, int64_t n,
+                cudaStream_t st);
+
+// Device state of a recorded FlexGMRES solve (FlexGMRES.cs:144-277 with Saad's least-squares update): the
+// Arnoldi index, the restart and Arnoldi loop conditions, the round-robin of the two preconditioners and the
+// stall fallback of the second, the Givens rotations and the residual history.
+struct FgState {
+  int j;          // Arnoldi column of the current step
+  int k1;         // j + 1: basis vectors the step projects against
+  int kk;         // columns of the finished cycle
+  int iter;       // preconditioner applications (ThisLevelIterations)
+  int outer;      // the restart loop continues
+  int inner;      // the Arnoldi loop continues
+  int use2;       // this step applies the second preconditioner
+  int nn_active;  // the second preconditioner is in use (off after a stall)
+  int turn;       // round-robin counter
+  int converged;
+  int nhist;      // entries written to the residual history
+  int stalled;    // the second preconditioner stalled in this solve
+  int started;    // r0 is set
+  int has2;       // a second preconditioner exists
+  int zero;       // constant 0 (slot index of the first basis vector)
+  int pad;
+  double r0, est, g_before, inv;  // inv: 1/|r| or 1/|w| for the next basis vector (0 when that norm is 0)
+};
+// Device arrays of the recorded FlexGMRES: Hessenberg matrix (row-major, m columns), rotations, right-hand side
+// of the least-squares problem, negated solution, residual history.
+struct FgArrays {
+  double* H;
+  double* cs;
+  double* sn;
+  double* g;
+  double* ny;
+  double* hist;
+  int m;
+  int hcap;
+};
+// start of a solve: counters cleared, nn_active / has2 as given
+void fg_begin(FgState* s, int nn_active, int has2, cudaStream_t st);
+// after a residual norm *rn: history, termination test (outer), the first Givens right-hand side g = (r, 0, ...)
+void fg_restart(FgState* s, FgArrays a, const double* rn, TermParams tp, int* err, cudaStream_t st);
+// start of an Arnoldi step: k1 = j + 1, which preconditioner it applies, |g_j| before it
+void fg_step_begin(FgState* s, FgArrays a, cudaStream_t st);
+// end of an Arnoldi step: Hessenberg column from the two projection sweeps h1, h2 and |w|, Givens rotation,
+// residual estimate, stall test of the second preconditioner, termination test (inner), j += 1
+void fg_step_end(FgState* s, FgArrays a, const double* h1, const double* h2, const double* wn, TermParams tp,
+                 double stall, int* err, cudaStream_t st);
+// back substitution of the finished cycle: ny = -H^{-1} g (kk columns)
+void fg_backsub(FgState* s, FgArrays a, cudaStream_t st);
+// out = tab[*idx] (idx null: slot 0)
+void slot_load(const double* const* tab, const int* idx, double* out, int64_t n, cudaStream_t st);
+// tab[*idx] = x * (*scale) (scale null: 1); an index outside 0..nslots-1 sets kDevErrSlots
+void slot_store(const double* x, const double* scale, double* const* tab, const int* idx, int nslots, int64_t n,
+                int* err, cudaStream_t st);
+
+// dst[i][0..n[i]) = src[i][0..n[i]) for i < count (the staging copies of a batch, one launch)
+void batch_copy(const double* const* src, double* const* dst, const int64_t* n, int count, cudaStream_t st);
+
 // y = x where *flag (vector copy predicated on a device flag)
 void copy_if(const double* x, double* y, int64_t n, const int* flag, cudaStream_t st);
 void copy_if(const float* x, float* y, int64_t n, const int* flag, cudaStream_t st);

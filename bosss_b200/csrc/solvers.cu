@@ -29,7 +29,7 @@ Ctx::~Ctx() {
 }
 
 namespace {
-constexpr int kMaxBodies = 8192;
+constexpr int kMaxBodies = 32768;
 constexpr int kMaxDepth = 16;
 }  // namespace
 
@@ -48,28 +48,63 @@ void Ctx::graph_init() {
   }
 }
 
-void Ctx::capture_begin() {
+// Conditional bodies keep their numbers across recordings (every recording appends its own), so that the execution
+// counters of a graph recorded earlier stay meaningful; body 0 counts the top level of the current recording.
+void Ctx::capture_join() {
   graph_init();
-  BSGPU_CUDA(cudaStreamSynchronize(st));
-  body_kernels.assign(1, 0);
-  body_names.assign(1, "top");
+  if (body_kernels.empty()) {
+    body_kernels.assign(1, 0);
+    body_names.assign(1, "top");
+  }
+  body_kernels[0] = 0;
+  first_body = (int)body_kernels.size();
   body_stack.clear();
   st_stack.clear();
   cur_body = 0;
-  BSGPU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
   capturing = true;
   mark = launches_now();
 }
 
-long long Ctx::capture_end(cudaGraph_t* g) {
+long long Ctx::recorded_total() const {
+  long long total = body_kernels[0];
+  for (size_t b = (size_t)first_body; b < body_kernels.size(); ++b) total += body_kernels[b];
+  return total;
+}
+
+long long Ctx::capture_leave() {
   require(st_stack.empty(), "graph capture: unbalanced conditional bodies");
   body_kernels[cur_body] += (long long)(launches_now() - mark);
   capturing = false;
-  BSGPU_CUDA(cudaStreamEndCapture(st, g));
-  long long total = 0;
-  for (long long k : body_kernels) total += k;
-  add_launches(-total);  // recorded, not launched: replays add what they run
+  add_launches(-recorded_total());  // recorded, not launched: replays add what they run
   return body_kernels[0];
+}
+
+void Ctx::capture_begin() {
+  graph_init();
+  BSGPU_CUDA(cudaStreamSynchronize(st));
+  capture_join();
+  BSGPU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+  mark = launches_now();
+}
+
+long long Ctx::capture_end(cudaGraph_t* g) {
+  const long long top = capture_leave();
+  BSGPU_CUDA(cudaStreamEndCapture(st, g));
+  return top;
+}
+
+void Ctx::capture_abort() {
+  while (!st_stack.empty()) {
+    cudaGraph_t b = nullptr;
+    cudaStreamEndCapture(st, &b);
+    st = st_stack.back();
+    st_stack.pop_back();
+  }
+  body_kernels[cur_body] += (long long)(launches_now() - mark);
+  add_launches(-recorded_total());
+  body_stack.clear();
+  cur_body = 0;
+  capturing = false;
 }
 
 int Ctx::new_body(const std::string& name) {
@@ -139,6 +174,7 @@ void Ctx::check_graph_errors() {
   BSGPU_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   BSGPU_CUDA(cudaStreamSynchronize(st));
   if (e & kDevErrSlots) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: history slots exhausted");
+  if (e & kDevErrKrylovNaN) throw Error(BSGPU_ERR_ARITHMETIC, "FlexGMRES: residual is NaN/Inf");
   if (e & kDevErrResidualIncrease) throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: residual increase");
   throw Error(BSGPU_ERR_ARITHMETIC, "Orthonormalization: NaN/Inf in the preconditioner");
 }
@@ -1618,6 +1654,17 @@ struct MixedAdapter : Solver<double> {
     this->converged = inner->converged;
     this->this_level_iterations = inner->this_level_iterations;
   }
+  bool graphable() const override { return inner->graphable(); }
+  void prepare_graph(Ctx& c) override { inner->prepare_graph(c); }
+  void solve_graph(Ctx& c, double* X, const double* B, bool zero) override {
+    convert(B, b32.p, N, c.st);
+    if (zero)
+      fill(0.0f, x32.p, N, c.st);
+    else
+      convert(X, x32.p, N, c.st);
+    inner->solve_graph(c, x32.p, b32.p, zero);
+    convert(x32.p, X, N, c.st);
+  }
 };
 
 // The p-multigrid V-cycle recorded once as a CUDA graph (device-side control flow, devctl.cuh) and replayed by one
@@ -1640,6 +1687,10 @@ struct GraphedT : Solver<T> {
     if (exec) cudaGraphExecDestroy(exec);
   }
   int nested() const override { return inner->this_level_iterations + inner->nested(); }
+  // inside a larger recording (the whole FlexGMRES solve) the V-cycle is recorded inline
+  bool graphable() const override { return inner->graphable(); }
+  void prepare_graph(Ctx& c) override { inner->prepare_graph(c); }
+  void solve_graph(Ctx& c, T* X, const T* B, bool zero) override { inner->solve_graph(c, X, B, zero); }
   void capture(Ctx& c, T* X, const T* B) {
     if (exec) {
       cudaGraphExecDestroy(exec);
@@ -1651,13 +1702,7 @@ struct GraphedT : Solver<T> {
     try {
       inner->solve_graph(c, X, B, true);
     } catch (...) {
-      while (!c.st_stack.empty()) {
-        cudaGraph_t b = nullptr;
-        cudaStreamEndCapture(c.st, &b);
-        c.st = c.st_stack.back();
-        c.st_stack.pop_back();
-      }
-      c.capturing = false;
+      c.capture_abort();
       cudaStreamEndCapture(c.st, &g);
       if (g) cudaGraphDestroy(g);
       throw;
@@ -1712,11 +1757,12 @@ struct GraphedT : Solver<T> {
 // tested after every Arnoldi step; the true residual is recomputed at every restart.  Arnoldi uses classical
 // Gram-Schmidt applied twice (one multi-dot and one multi-axpy launch per sweep) instead of MGS.
 // ---------------------------------------------------------------------------------------------------------------
-struct FlexGMRES : Solver<double> {
+struct FlexGMRES : Solver<double>, RecordedSolve {
   const Matrix* A;
   int64_t N;
   int m;
   Term term;
+  bool whole = false;  // cfg.graph == 2: the handle records the whole solve (RecordedSolve)
   std::unique_ptr<Solver<double>> pc;
   // second preconditioner used in turn with pc (FlexGMRES.cs:196-199 cycles PrecondS); switched off for the rest
   // of a solve when one of its steps reduces the residual estimate by less than the factor `stall`
@@ -1848,7 +1894,149 @@ struct FlexGMRES : Solver<double> {
       axpys(kk, nullptr, y.data(), 1.0, zx.data(), X, N, c.st);
     }
   }
+
+  // ---- the recorded whole solve (RecordedSolve) ----
+  // Same steps as solve() with the host's scalars and branches moved to FgState: the basis vectors and the
+  // preconditioned vectors are addressed through device pointer tables by the device's Arnoldi index (slot_load /
+  // slot_store), the Gram-Schmidt sweeps project against the first j + 1 basis vectors with hist_dots /
+  // hist_axpy1, and the cycle's update X += Z y is one hist_axpy1 with the negated back-substitution.
+  DBuf<double> vin, zf, Wf, farr;
+  DBuf<double*> dV, dZ;
+  HistScratch hsV;
+  DBuf<FgState> fst;
+  FgArrays fa{};
+  double *d_h1 = nullptr, *d_h2 = nullptr, *d_wn = nullptr, *d_rn = nullptr;
+  FgState* h_fst = nullptr;
+  double* h_hist = nullptr;
+  ~FlexGMRES() override {
+    if (h_fst) cudaFreeHost(h_fst);
+    if (h_hist) cudaFreeHost(h_hist);
+  }
+  void norm_dev(Ctx& c, const double* v, double* out) {
+    const double* a[1] = {v};
+    dots(c.red, 1, a, a, N, out, 1, c.st);
+  }
+  void prepare(Ctx& c) override {
+    if (!fst.p) {
+      require(m + 1 <= kHistMax, "recorded FlexGMRES: MaxKrylovDim above 127", BSGPU_ERR_UNSUPPORTED);
+      const int64_t n1 = std::max<int64_t>(N, 1);
+      vin.alloc(n1);
+      zf.alloc(n1);
+      Wf.alloc(n1);
+      std::vector<double*> pv(m + 1), pz(m);
+      for (int j = 0; j <= m; ++j) pv[j] = V[j].p;
+      for (int j = 0; j < m; ++j) pz[j] = Z[j].p;
+      dV.alloc(m + 1);
+      dZ.alloc(m);
+      BSGPU_CUDA(cudaMemcpy(dV.p, pv.data(), (m + 1) * sizeof(double*), cudaMemcpyHostToDevice));
+      BSGPU_CUDA(cudaMemcpy(dZ.p, pz.data(), m * sizeof(double*), cudaMemcpyHostToDevice));
+      hsV.init(m + 1);
+      fst.alloc(1);
+      BSGPU_CUDA(cudaMemset(fst.p, 0, sizeof(FgState)));
+      fa.m = m;
+      fa.hcap = 2 * std::max(term.max_iter, 1) + 16;
+      const size_t nH = (size_t)(m + 1) * m;
+      farr.alloc(nH + 3 * (size_t)m + (m + 1) + fa.hcap);
+      BSGPU_CUDA(cudaMemset(farr.p, 0, (nH + 3 * (size_t)m + (m + 1) + fa.hcap) * sizeof(double)));
+      fa.H = farr.p;
+      fa.cs = fa.H + nH;
+      fa.sn = fa.cs + m;
+      fa.ny = fa.sn + m;
+      fa.g = fa.ny + m;
+      fa.hist = fa.g + (m + 1);
+      d_h1 = c.scal(m + 1);
+      d_h2 = c.scal(m + 1);
+      d_wn = c.scal(1);
+      d_rn = c.scal(1);
+      BSGPU_CUDA(cudaMallocHost(&h_fst, sizeof(FgState)));
+      BSGPU_CUDA(cudaMallocHost(&h_hist, fa.hcap * sizeof(double)));
+    }
+    c.graph_init();
+    require(pc && pc->graphable() && (!pc2 || pc2->graphable()),
+            "the FlexGMRES solve cannot be recorded as a graph with this preconditioner", BSGPU_ERR_UNSUPPORTED);
+    pc->prepare_graph(c);
+    if (pc2) pc2->prepare_graph(c);
+  }
+  // the learned stage (second preconditioner or pre-smoother inside the V-cycle) switched on or off
+  int key() const override { return (tree && tree->net && tree->learned_on) ? 1 : 0; }
+  void precondition_dev(Ctx& c, Solver<double>* p) {
+    fill(0.0, zf.p, N, c.st);
+    p->solve_graph(c, zf.p, vin.p, true);
+  }
+  void record(Ctx& c, double* X, const double* B) override {
+    const TermParams tp = term.params();
+    FgState* s = fst.p;
+    const std::string tag = this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string("FlexGMRES: ");
+    fg_begin(s, (pc2 && key()) ? 1 : 0, pc2 ? 1 : 0, c.st);
+    spmv(*A, -1.0, X, 1.0, B, R0.p, c.st);
+    norm_dev(c, R0.p, d_rn);
+    fg_restart(s, fa, d_rn, tp, c.d_err, c.st);
+    const cudaGraphConditionalHandle h_outer = c.cond_handle();
+    const int b_outer = c.new_body(tag + "restart cycle");
+    cond_set(h_outer, &s->outer, nullptr, nullptr, 0, c.exec_of(b_outer), c.st);
+    c.cond_begin(h_outer, cudaGraphCondTypeWhile, b_outer);
+    {
+      slot_store(R0.p, &s->inv, dV.p, nullptr, m + 1, N, c.d_err, c.st);
+      const cudaGraphConditionalHandle h_inner = c.cond_handle();
+      const int b_inner = c.new_body(tag + "Arnoldi step");
+      cond_set(h_inner, &s->inner, nullptr, nullptr, 0, c.exec_of(b_inner), c.st);
+      c.cond_begin(h_inner, cudaGraphCondTypeWhile, b_inner);
+      {
+        fg_step_begin(s, fa, c.st);
+        slot_load(dV.p, &s->j, vin.p, N, c.st);
+        if (pc2) {
+          const cudaGraphConditionalHandle h1 = c.cond_handle();
+          const int b1 = c.new_body(tag + "first preconditioner");
+          cond_set(h1, nullptr, &s->use2, nullptr, 0, c.exec_of(b1), c.st);
+          c.cond_begin(h1, cudaGraphCondTypeIf, b1);
+          precondition_dev(c, pc.get());
+          c.cond_end();
+          const cudaGraphConditionalHandle h2 = c.cond_handle();
+          const int b2 = c.new_body(tag + "second preconditioner");
+          cond_set(h2, &s->use2, nullptr, nullptr, 0, c.exec_of(b2), c.st);
+          c.cond_begin(h2, cudaGraphCondTypeIf, b2);
+          precondition_dev(c, pc2.get());
+          c.cond_end();
+        } else {
+          precondition_dev(c, pc.get());
+        }
+        slot_store(zf.p, nullptr, dZ.p, &s->j, m, N, c.d_err, c.st);
+        spmv(*A, 1.0, zf.p, 0.0, (const double*)nullptr, Wf.p, c.st);
+        hist_dots(hsV, dV.p, &s->k1, Wf.p, N, d_h1, nullptr, c.st);
+        hist_axpy1(dV.p, &s->k1, m + 1, d_h1, Wf.p, N, c.st);
+        hist_dots(hsV, dV.p, &s->k1, Wf.p, N, d_h2, nullptr, c.st);
+        hist_axpy1(dV.p, &s->k1, m + 1, d_h2, Wf.p, N, c.st);
+        norm_dev(c, Wf.p, d_wn);
+        fg_step_end(s, fa, d_h1, d_h2, d_wn, tp, stall, c.d_err, c.st);
+        slot_store(Wf.p, &s->inv, dV.p, &s->j, m + 1, N, c.d_err, c.st);
+        cond_set(h_inner, &s->inner, nullptr, nullptr, 0, c.exec_of(b_inner), c.st);
+      }
+      c.cond_end();
+      fg_backsub(s, fa, c.st);
+      hist_axpy1(dZ.p, &s->kk, m, fa.ny, X, N, c.st);
+      spmv(*A, -1.0, X, 1.0, B, R0.p, c.st);
+      norm_dev(c, R0.p, d_rn);
+      fg_restart(s, fa, d_rn, tp, c.d_err, c.st);
+      cond_set(h_outer, &s->outer, nullptr, nullptr, 0, c.exec_of(b_outer), c.st);
+    }
+    c.cond_end();
+  }
+  void queue_result(Ctx& c, cudaStream_t st) override {
+    BSGPU_CUDA(cudaMemcpyAsync(h_fst, fst.p, sizeof(FgState), cudaMemcpyDeviceToHost, st));
+    BSGPU_CUDA(cudaMemcpyAsync(h_hist, fa.hist, fa.hcap * sizeof(double), cudaMemcpyDeviceToHost, st));
+    BSGPU_CUDA(cudaMemcpyAsync(c.h_err, c.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    c.err_pending = true;
+  }
+  void take_result(Ctx& c) override {
+    (void)c;
+    const FgState& s = *h_fst;
+    this->history.assign(h_hist, h_hist + std::min(std::max(s.nhist, 0), fa.hcap));
+    this->this_level_iterations = s.iter;
+    this->converged = s.converged != 0;
+    if (s.stalled && tree) tree->learned_stalls++;
+  }
 };
+
 
 // ---------------------------------------------------------------------------------------------------------------
 // SoftGMRES.Solve (SoftGMRES.cs:227-460): restarted GMRES(m) with left preconditioning, r = M^{-1}(b - A x),
@@ -2210,6 +2398,11 @@ std::unique_ptr<Solver<T>> build_level(Tree& t, const Matrix* A64, const Matrix*
 
 }  // namespace
 
+RecordedSolve* recorded_form(Tree& t) {
+  auto* f = dynamic_cast<FlexGMRES*>(t.top.get());
+  return (f && f->whole) ? static_cast<RecordedSolve*>(f) : nullptr;
+}
+
 Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info) {
   require(!A->single, "the solver operator must be FP64");
   require(cfg.n_levels >= 1 && cfg.n_levels <= 8, "n_levels must be in 1..8");
@@ -2234,6 +2427,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
       require(cfg.level_keep[l] >= 1 && cfg.level_keep[l] < cfg.level_keep[l - 1], "level_keep must decrease");
   }
   const bool mixed = cfg.precision == BSGPU_PRECISION_MIXED;
+  require(cfg.graph >= 0 && cfg.graph <= 2, "graph must be 0, 1 or 2");
   if (cfg.learned != BSGPU_LEARNED_OFF) {
     require(cfg.solver == BSGPU_SOLVER_FGMRES_PMG, "the learned stage needs the FGMRES + p-multigrid solver");
     require(info.nbr != nullptr && info.nfaces > 0, "the learned stage needs the cell graph (bsgpu_mgop_set_cell_neighbours)");
@@ -2280,7 +2474,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
           g->Xs = ad->x32.p;
           g->Bs = ad->b32.p;
           g->key_src = &t->learned_on;
-          g->ensure(*t->ctx);  // recorded at set-up, not in the first solve
+          if (cfg.graph == 1) g->ensure(*t->ctx);  // recorded at set-up, not in the first solve
           ad->inner = std::move(g);
         } else {
           ad->inner = std::move(lvl);
@@ -2293,7 +2487,7 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
                   BSGPU_ERR_UNSUPPORTED);
           auto g = std::make_unique<GraphedT<double>>(A->N, std::move(lvl));
           g->key_src = &t->learned_on;
-          g->ensure(*t->ctx);  // recorded at set-up, not in the first solve
+          if (cfg.graph == 1) g->ensure(*t->ctx);  // recorded at set-up, not in the first solve
           f->pc = std::move(g);
         } else {
           f->pc = std::move(lvl);
@@ -2305,6 +2499,8 @@ Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const Operator
         f->pc2->trace = t->ctx->trace_id("LearnedStage");
         f->stall = cfg.learned_stall > 0 ? cfg.learned_stall : 0.99;
       }
+      // cfg.graph == 2: the handle records the whole solve (recorded_form) at set-up
+      f->whole = cfg.graph == 2;
       t->top = std::move(f);
       break;
     }

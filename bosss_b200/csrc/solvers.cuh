@@ -76,6 +76,14 @@ struct Ctx {
   void graph_init();
   void capture_begin();
   long long capture_end(cudaGraph_t* g);  // returns the kernels recorded at the top level
+  // recording into a graph whose capture another stream began (st joined it through an event): the same
+  // bookkeeping without beginning or ending the capture of st
+  void capture_join();
+  long long capture_leave();
+  int first_body = 1;                   // first conditional body of the current recording
+  long long recorded_total() const;     // kernels recorded by the current recording
+  // after an exception inside a recording: ends the open conditional bodies and leaves capturing mode
+  void capture_abort();
   int new_body(const std::string& name);
   std::vector<std::string> body_names;
   std::map<std::string, unsigned long long> graph_counts;  // executions of the conditional bodies, by name
@@ -159,6 +167,20 @@ struct Tree {
   int learned_pool = 0;             // training residuals collected by the last train_learned
 };
 Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info);
+
+// The whole FlexGMRES solve recorded into a CUDA graph (cfg.graph == 2): restart and Arnoldi loops as WHILE nodes,
+// the preconditioners' round-robin as IF nodes, every decision on the device (devctl.cuh FgState), the V-cycle
+// recorded inline.  Used by the solver handle (one graph per handle) and by batches (one graph for many handles).
+struct RecordedSolve {
+  virtual ~RecordedSolve() {}
+  virtual void prepare(Ctx& c) = 0;                           // buffers and the preconditioners' recorded forms
+  virtual void record(Ctx& c, double* X, const double* B) = 0;  // emits the solve into the capture on c.st
+  virtual int key() const = 0;                                // changes when the recording must be redone
+  virtual void queue_result(Ctx& c, cudaStream_t st) = 0;     // device state -> pinned host memory on st
+  virtual void take_result(Ctx& c) = 0;                       // after st synchronised: iterations, history, ...
+};
+// the recorded form of the tree's top solver, or nullptr (not FlexGMRES, or cfg.graph != 2)
+RecordedSolve* recorded_form(Tree& t);
 // Generates training residuals with the solver itself (FGMRES Arnoldi vectors of solves with seeded random
 // right-hand sides, learned stage off) and trains the learned stage; returns the final mean loss.
 double train_learned(Tree& t, int n_rhs, int steps, double lr, uint64_t seed);

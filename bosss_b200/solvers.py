@@ -335,7 +335,9 @@ class FGMRESConfig(IterativeSolverConfig):
     LearnedHidden: int = 64
     LearnedStall: float = 0.99
     LearnedPairs: int = 0           # training residuals collected in total (0: 12 per right-hand side)
-    Graph: bool = False             # record the V-cycle once as a CUDA graph with device-side decisions
+    # True / "vcycle": record the V-cycle once as a CUDA graph with device-side decisions; "solve": record the
+    # whole solve (FlexGMRES loops included) as one graph, one launch per solve, usable in a GpuBatch
+    Graph: object = False
     Autotune: bool = False          # time the launch shapes of the level matrices' kernels at set-up
 
     def _config(self):
@@ -356,7 +358,10 @@ class FGMRESConfig(IterativeSolverConfig):
         if self.LearnedPairs < 0:
             raise ValueError("LearnedPairs must be >= 0")
         c.learned_pairs = self.LearnedPairs
-        c.graph = 1 if self.Graph else 0
+        graph_modes = {False: 0, None: 0, "off": 0, True: 1, "vcycle": 1, "solve": 2}
+        if self.Graph not in graph_modes:
+            raise ValueError("Graph must be False, True / 'vcycle' or 'solve'")
+        c.graph = graph_modes[self.Graph]
         c.autotune = 1 if self.Autotune else 0
         return c
 
@@ -598,6 +603,56 @@ class GpuSolver:
         if self._h is not None:
             nat.lib().bsgpu_solver_destroy(self._h)
         self._h = None
+
+    def __del__(self):
+        try:
+            self.Dispose()
+        except Exception:
+            pass
+
+
+class GpuBatch:
+    """Independent systems solved together from ONE CUDA graph (bsgpu_batch_*): every member's whole solve
+    (``FGMRESConfig(Graph="solve")``) is one branch of the graph, all branches run concurrently from one launch.
+    The reference solves independent systems one after another (``UniSolver.cs:588,623``)."""
+
+    def __init__(self, solvers: List["GpuSolver"]):
+        if not solvers:
+            raise ValueError("empty batch")
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_batch_create(C.byref(h), arr, len(self.solvers)))
+        self._h = h
+        self.stats = (nat.SolveStats * len(self.solvers))()
+
+    def Solve(self, Xs, Bs):
+        """Xs: initial guesses in, solutions out; Bs: right-hand sides (device tensors, original basis)."""
+        n = len(self.solvers)
+        if len(Xs) != n or len(Bs) != n:
+            raise ValueError("one X and one B per batch member")
+        for s, X, B in zip(self.solvers, Xs, Bs):
+            if not (_is_device(X) and _is_device(B)):
+                raise ValueError("batch vectors must be device tensors")
+            N = s.op.BaseMatrix.N
+            if X.numel() != N or B.numel() != N:
+                raise ValueError("Wrong length of unknowns or RHS vector.")
+        xp = (C.c_void_p * n)(*[nat.ptr(X) for X in Xs])
+        bp = (C.c_void_p * n)(*[nat.ptr(B) for B in Bs])
+        rc = nat.lib().bsgpu_batch_solve_device(self._h, xp, bp, self.stats)
+        for s, st in zip(self.solvers, self.stats):  # results are written even when a member raised
+            C.memmove(C.byref(s.stats), C.byref(st), C.sizeof(st))
+        nat.check(rc)
+        return Xs
+
+    def Latencies(self) -> List[float]:
+        """Device seconds from the batch launch to the end of each member's solve."""
+        return [st.seconds for st in self.stats]
+
+    def Dispose(self):
+        if getattr(self, "_h", None):
+            nat.lib().bsgpu_batch_destroy(self._h)
+            self._h = None
 
     def __del__(self):
         try:

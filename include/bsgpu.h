@@ -203,7 +203,10 @@ typedef struct {
                                n_rhs solves (0: 12 per right-hand side)                           */
   int32_t graph;            /* 1: record the p-multigrid V-cycle of BSGPU_SOLVER_FGMRES_PMG once as a CUDA graph
                                with its decisions (termination tests, re-orthonormalisation, residual checks) taken
-                               on the device, and replay it per application; 0: host-driven (default)       */
+                               on the device, and replay it per application; 2: record the whole solve (change of
+                               basis, FlexGMRES restart and Arnoldi loops, Givens rotations, preconditioner
+                               round-robin, V-cycle) as one graph, replayed by one launch per solve and usable in a
+                               bsgpu_batch; 0: host-driven (default).  Tracing and training run host-driven. */
   int32_t autotune;         /* 1: pick the launch shape (threads per CTA) of every level matrix's product and
                                block-Jacobi kernels by timing the candidates at set-up (bsgpu_autotune_report) */
   int32_t fp16_storage;     /* BSGPU_FP16_* bits, with BSGPU_PRECISION_MIXED: parts of the FP32 preconditioner
@@ -246,6 +249,21 @@ BSGPU_API int bsgpu_solver_set_tracing(bsgpu_solver_t s, int32_t on);
 BSGPU_API int bsgpu_solver_train_learned(bsgpu_solver_t s, int32_t n_rhs, int32_t steps, double lr, uint64_t seed,
                                          double* loss);
 BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len);
+
+/* ---- batches of independent systems (no counterpart in the reference, which solves them one after another,
+ * UniSolver.cs:588,623) ----------------------------------------------------------------------------------------- *
+ * create records the whole solves of n handles (each created with cfg.graph = 2, each at most once in the batch) as
+ * the branches of ONE CUDA graph; solve_device stages B[i] and the initial guess X[i] (device vectors) into handle
+ * i's buffers, runs every member concurrently from one graph launch, writes the solutions to X[i] and returns when
+ * all are done.  stats (n entries, may be NULL): per member as bsgpu_solver_solve_device, with seconds = device time
+ * from the launch to the end of that member's branch (its latency inside the batch).  The member handles must not
+ * be used elsewhere while a batch solve runs; a batch whose member had its learned stage switched since create is
+ * rejected (create it again).  Errors a member's solve records are raised after all results were written. */
+typedef struct bsgpu_batch_s* bsgpu_batch_t;
+BSGPU_API int bsgpu_batch_create(bsgpu_batch_t* b, const bsgpu_solver_t* solvers, int32_t n);
+BSGPU_API int bsgpu_batch_solve_device(bsgpu_batch_t b, double* const* X, const double* const* B,
+                                       bsgpu_solve_stats* stats);
+BSGPU_API int bsgpu_batch_destroy(bsgpu_batch_t b);
 
 /* ---- learned stage access (no counterpart in the reference) --------------------------------------------- *
  * For checking and exchanging the trained network.  dims[8]: Np, nfaces, nextra, F (input width), Fp (F padded

@@ -42,3 +42,13 @@ def test_softgmres_and_softpcg_mapping():
     with pytest.raises(ValueError):
         SoftGMRESConfig(Precond="amg")._config()
     assert SoftPCGConfig(BlockJacobiPrecond=False)._config().bj_iters == -1
+
+
+@pytest.mark.parametrize("graph,value", [(False, 0), (True, 1), ("vcycle", 1), ("solve", 2)])
+def test_fgmres_graph_modes(graph, value):
+    assert FGMRESConfig(Graph=graph)._config().graph == value
+
+
+def test_fgmres_rejects_unknown_graph_mode():
+    with pytest.raises(ValueError):
+        FGMRESConfig(Graph="always")._config()
