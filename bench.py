@@ -75,6 +75,11 @@ def parse():
     return args
 
 
+def learned_rhs_count(iterations: int, pairs: int = 200) -> int:
+    """Training solves needed to collect `pairs` Arnoldi vectors at `iterations` per solve (at most 25)."""
+    return max(2, min(25, -(-pairs // max(1, int(iterations))) + 1))
+
+
 def levels_for(p: int):
     from bosss_b200.assembly import np_of
     return tuple(np_of(3, q) for q in range(p, 0, -1))
@@ -422,10 +427,12 @@ def run_ours(args):
         slv.Dispose()
     if args.learned_variant:
         # the learned stage (FGMRES round-robin and pre-smoother) on top of the fast form, trained on 200
-        # residuals the solver generates (the Arnoldi vectors of 5 solves with seeded right-hand sides)
+        # residuals the solver generates (the Arnoldi vectors of solves with seeded right-hand sides: enough solves
+        # of the fast form's iteration count to collect 200)
         op.SetCellGraph(s.grid.face_neighbours())
+        n_rhs = learned_rhs_count(fast_iters)
         slv, t_set = timed_setup(lambda: mk(True, args.graph, args.autotune, learned="both", fp16=args.fp16))
-        _, t_train = timed_setup(lambda: slv.TrainLearned(n_rhs=5, steps=400, lr=2e-3, seed=1))
+        _, t_train = timed_setup(lambda: slv.TrainLearned(n_rhs=n_rhs, steps=400, lr=2e-3, seed=1))
         t = time_variant(slv)
         variants["learned_mixed"] = {"value": max_over_ranks(t, ws), "unit": "s", "iters": slv.ThisLevelIterations,
                                      "setup_s": t_set, "train_s": t_train, "pairs": slv.LearnedInfo()["pairs"],
@@ -627,7 +634,7 @@ def run_single_system(args, s, workload, prepare=None):
     fast_setup = time.perf_counter() - t0
     if args.learned != "off":
         t0 = time.perf_counter()
-        fast.TrainLearned(n_rhs=5, steps=400, lr=2e-3, seed=1)
+        fast.TrainLearned(n_rhs=learned_rhs_count(res[fast_name]["iters"]), steps=400, lr=2e-3, seed=1)
         torch.cuda.synchronize()
         train_s = time.perf_counter() - t0
     for _ in range(args.warmup):

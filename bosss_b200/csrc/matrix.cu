@@ -7,6 +7,7 @@
 
 #include "ldst.cuh"
 #include "matrix.cuh"
+#include "reduce.cuh"
 
 namespace bsgpu {
 
@@ -167,6 +168,62 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
       y[g] = fma(alpha, s0 + s1, x[g]);
     }
   }
+}
+
+// CG search direction and its image in one pass (uniform blocks): p_new = z + beta p_old, q = A p_new, and
+// sigma = p_new . q as a grid reduction.  The gathered entries of p_new are formed on the fly from z and p_old, so
+// p_old stays readable by every CTA while each CTA writes its own rows of p_new (a second buffer), and the separate
+// direction update and dot product launches of the textbook iteration disappear.  The arithmetic of p_new and of
+// the row products is that of xpby followed by the uniform SpMV.
+template <typename T, int NP, int V>
+__global__ void __launch_bounds__(256) cg_direction_kernel(
+    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const T* __restrict__ vals,
+    const T* __restrict__ z, const T* __restrict__ pold, T* __restrict__ pnew, T* __restrict__ q,
+    const double* __restrict__ beta_p, int64_t nb, const int* __restrict__ active, double* __restrict__ partial,
+    unsigned int* __restrict__ ticket, double* __restrict__ sigma) {
+  static_assert(NP % V == 0, "chunk width must divide the block size");
+  if (*active == 0) return;
+  constexpr int BPC = 256 / NP;
+  const double beta = *beta_p;
+  const int t = threadIdx.x;
+  const int lb = t / NP;
+  const int r = t - lb * NP;
+  const uint64_t pol = policy_evict_first();
+  double acc[1] = {0.0};
+  for (int64_t tile = blockIdx.x; tile * BPC < nb; tile += gridDim.x) {
+    const int64_t i = tile * BPC + lb;
+    if (lb < BPC && i < nb) {
+      T a0 = 0, a1 = 0;
+      const int64_t k0 = rp[i], k1 = rp[i + 1];
+      for (int64_t k = k0; k < k1; ++k) {
+        const int64_t j = ci[k];
+        const T* vb = vals + k * (NP * NP) + r * V;
+        const T* zb = z + j * NP;
+        const T* pb = pold + j * NP;
+#pragma unroll
+        for (int c = 0; c < NP / V; ++c) {
+          Vec<T, V> a = ldv_stream<T, V>(vb + c * (NP * V), pol);
+          Vec<T, V> zv = ldv_cached<T, V>(zb + c * V);
+          Vec<T, V> pv = ldv_cached<T, V>(pb + c * V);
+#pragma unroll
+          for (int e = 0; e < V; ++e) {
+            const T xv = (T)((double)zv.a[e] + beta * (double)pv.a[e]);
+            if ((c * V + e) & 1)
+              a1 = fma(a.a[e], xv, a1);
+            else
+              a0 = fma(a.a[e], xv, a0);
+          }
+        }
+      }
+      const int64_t g = i * NP + r;
+      const T qv = a0 + a1;
+      const T pn = (T)((double)z[g] + beta * (double)pold[g]);
+      pnew[g] = pn;
+      q[g] = qv;
+      acc[0] = fma((double)pn, (double)qv, acc[0]);
+    }
+  }
+  gridred::finish_dots<1>(acc, 1, partial, ticket, sigma, 0);
 }
 
 // General block sizes (XDG: 1..n species per block).  CTA b owns DOF rows cta_row0[b] .. cta_row0[b+1]-1,
@@ -754,6 +811,44 @@ void spmv(const Matrix& A, float alpha, const float* x, float beta, const float*
   check_aligned(x, 16, "x");
   if (A.half) return dispatch_half<0>(A, x, z, y, alpha, beta, nullptr, st, active);
   dispatch<float, 0>(A, A.v32.p, x, z, y, alpha, beta, nullptr, nullptr, st, active);
+}
+
+namespace {
+template <typename T>
+bool cg_direction_impl(const Matrix& A, const T* vals, const T* z, const T* pold, T* pnew, T* q, const double* beta,
+                       double* sigma, ReduceScratch& red, const int* active, cudaStream_t st) {
+  if (!specialised(A) || A.half || A.nb == 0) return false;
+  check_aligned(z, 16, "z");
+  check_aligned(pold, 16, "p");
+  if (!red.grid) red.init();
+  constexpr int VW = sizeof(T) == 8 ? 2 : 4;
+#define BSGPU_CGD(NP, VV)                                                                                       \
+  cg_direction_kernel<T, NP, VV><<<(unsigned)std::min<int64_t>((A.nb + 256 / NP - 1) / (256 / NP), red.grid),     \
+                                   256, 0, st>>>(A.rp.p, A.ci.p, vals, z, pold, pnew, q, beta, A.nb, active,      \
+                                                 red.partial.p, red.ticket.p, sigma)
+  switch (A.Np) {
+    case 20: BSGPU_CGD(20, VW); break;
+    case 4: BSGPU_CGD(4, VW); break;
+    case 10: BSGPU_CGD(10, 2); break;
+    default: BSGPU_CGD(6, 2); break;
+  }
+#undef BSGPU_CGD
+  BSGPU_CHECK_LAUNCH();
+  return true;
+}
+}  // namespace
+
+bool cg_direction_supported(const Matrix& A) { return specialised(A) && !A.half && A.nb > 0; }
+
+bool cg_direction(const Matrix& A, const double* z, const double* pold, double* pnew, double* q, const double* beta,
+                  double* sigma, ReduceScratch& red, const int* active, cudaStream_t st) {
+  require(!A.single, "FP64 CG direction on an FP32 matrix");
+  return cg_direction_impl<double>(A, A.v64.p, z, pold, pnew, q, beta, sigma, red, active, st);
+}
+bool cg_direction(const Matrix& A, const float* z, const float* pold, float* pnew, float* q, const double* beta,
+                  double* sigma, ReduceScratch& red, const int* active, cudaStream_t st) {
+  require(A.single, "FP32 CG direction on an FP64 matrix");
+  return cg_direction_impl<float>(A, A.v32.p, z, pold, pnew, q, beta, sigma, red, active, st);
 }
 
 namespace {

@@ -48,7 +48,9 @@ def test_recorded_solve_matches_host_flexgmres(cuda, mixed):
     hh, hr = host.History(), rec.History()
     assert abs(len(hr) - len(hh)) <= 1
     assert abs(hr[0] - hh[0]) <= 1e-12 * hh[0]
-    assert hr[-1] <= 1e-12 * hr[0]
+    # the last entry is the true residual of the final restart test: below tol * r0 or the absolute floor 2.2e-13
+    # of DefaultTermination (IterativeSolverConfig.cs:48-62)
+    assert hr[-1] <= max(1e-12 * hr[0], 2.2205e-13)
     # replayed kernels are counted (the same order as the host-driven solve)
     assert 0.5 * nh <= nr <= 2.0 * nh, (nh, nr)
     # a second solve replays the recording; device vectors take the same path
@@ -100,10 +102,11 @@ def test_recorded_solve_tracing_runs_host_driven(cuda):
     it = rec.ThisLevelIterations
     rec.SetTracing(True)
     xt, _ = _solve(rec, s)
+    trace = rec.Trace()
     rec.SetTracing(False)
     assert abs(rec.ThisLevelIterations - it) <= 1
     assert np.linalg.norm(xt - xr) <= 1e-9 * np.linalg.norm(xr)
-    assert any(t["name"] == "FlexGMRES" and t["calls"] > 0 for t in rec.Trace())
+    assert any(t["name"] == "FlexGMRES" and t["calls"] > 0 for t in trace)
 
 
 def test_recorded_solve_learned_round_robin(cuda):
