@@ -57,6 +57,8 @@ def parse():
                          "k = exp(GRF) diffusion, 96^3 p=2; xdgbatch: 256 independent sphere problems")
     ap.add_argument("--batch", type=int, default=256, help="xdgbatch: number of problems")
     ap.add_argument("--concurrency", type=int, default=16, help="xdgbatch: problems solved at once")
+    ap.add_argument("--batch-order", default="size", choices=["size", "given"],
+                    help="xdgbatch: waves of problems sorted by size and jump (largest first) or in seed order")
     ap.add_argument("--learned", default="off", help="varcoef96/xdgbatch: learned stage mode")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="fast form without graph recording")
@@ -416,7 +418,7 @@ def run_ours(args):
     # 4. other forms, for the attribution of the speed-up (each: set-up, one warm-up, best of two)
     variants = {}
     forms = {"fp64_graph": dict(mixed=False, graph=True, tune=args.autotune),
-             "mixed_host": dict(mixed=True)}
+             "mixed_host": dict(mixed=True, tune=args.autotune)}
     for name, kw in forms.items():
         slv, t_set = timed_setup(lambda: mk(**kw))
         torch.cuda.nvtx.range_push("variant_" + name)
@@ -804,6 +806,9 @@ def run_xdg_batch(args):
     specs = xdg.batch_specs(args.batch, seed=args.seed)
     from bosss_b200 import replicas
     mine = [specs[i] for i in replicas.shard(len(specs), ws, rank)]
+    if args.batch_order == "size":
+        # longest-first scheduling: waves of similar problems (grid size, then diffusivity jump) finish together
+        mine.sort(key=lambda sp: (sp["n"], sp["mu"][1]), reverse=True)
     procs = max(1, min(16, (os.cpu_count() or 2) // max(ws, 1) - 1))
     pool = mp.get_context("spawn").Pool(procs)
     import torch
@@ -833,6 +838,7 @@ def run_xdg_batch(args):
         "vs_baseline": None, "dtype": "f64 (outer) / f32 (preconditioner)", "data": "synthetic (seeded problems)",
         "config": {"workload": f"{args.batch} {XDGBATCH}", "concurrency": args.concurrency, "tol": TOL,
                    "parallelism": f"replicas x{ws} (problems sharded)", "host_generation_procs": procs,
+                   "order": args.batch_order,
                    "fast_graph": args.graph, "fast_wave": "one graph launch" if args.graph == "solve" else
                    "host threads, one stream per problem"},
         "fast": fast, "plain_fp64": plain, "plain_fp64_dof_per_s": agg_plain["per_s"],

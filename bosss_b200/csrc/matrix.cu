@@ -300,9 +300,8 @@ __global__ void __launch_bounds__(256) spmv_general_kernel(
 // so no chunk straddles a species boundary and there is no scalar tail).
 template <typename T, int NP, int NS, int V, int MODE>
 __device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, const int32_t* __restrict__ rows,
-                                           const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                           const int32_t* __restrict__ len, const int64_t* __restrict__ i0,
-                                           const int64_t* __restrict__ boff, const T* __restrict__ vals,
+                                           const int64_t* __restrict__ rp, const TypedBlock* __restrict__ tb,
+                                           const int64_t* __restrict__ i0, const T* __restrict__ vals,
                                            const T* __restrict__ x, const T* __restrict__ z, T* __restrict__ y,
                                            T alpha, T beta, const T* __restrict__ dinv,
                                            const int64_t* __restrict__ doff) {
@@ -319,10 +318,10 @@ __device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, c
   if (valid) {
     const int64_t k0 = rp[i], k1 = rp[i + 1];
     for (int64_t k = k0; k < k1; ++k) {
-      const int64_t j = ci[k];
-      const int sj = len[j] / NP;
-      const T* vb = vals + boff[k] + r * V;
-      const T* xb = x + i0[j];
+      const TypedBlock m = tb[k];
+      const int sj = m.nsp;
+      const T* vb = vals + m.boff + r * V;
+      const T* xb = x + m.xoff;
       for (int sp = 0; sp < sj; ++sp) {
 #pragma unroll
         for (int c = 0; c < NP / V; ++c) {
@@ -369,19 +368,19 @@ __device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, c
 // One launch for both species counts: CTAs [0, cta1) take the one-species rows, the rest the two-species rows.
 template <typename T, int NP, int V, int MODE>
 __global__ void __launch_bounds__(256) spmv_typed_kernel(
-    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const int32_t* __restrict__ len,
-    const int64_t* __restrict__ i0, const int64_t* __restrict__ boff, const int32_t* __restrict__ rows,
+    const int64_t* __restrict__ rp, const TypedBlock* __restrict__ tb, const int64_t* __restrict__ i0,
+    const int32_t* __restrict__ rows,
     int64_t n1, int64_t n2, int64_t cta1, const T* __restrict__ vals, const T* __restrict__ x,
     const T* __restrict__ z, T* __restrict__ y, T alpha, T beta, const T* __restrict__ dinv,
     const int64_t* __restrict__ doff, const int* __restrict__ active) {
   if (active != nullptr && *active == 0) return;
   const int bpc1 = blockDim.x / NP, bpc2 = blockDim.x / (2 * NP);
   if ((int64_t)blockIdx.x < cta1)
-    typed_rows<T, NP, 1, V, MODE>(bpc1, (int64_t)blockIdx.x * bpc1, n1, rows, rp, ci, len, i0, boff, vals, x, z, y,
-                                  alpha, beta, dinv, doff);
+    typed_rows<T, NP, 1, V, MODE>(bpc1, (int64_t)blockIdx.x * bpc1, n1, rows, rp, tb, i0, vals, x, z, y, alpha,
+                                  beta, dinv, doff);
   else
-    typed_rows<T, NP, 2, V, MODE>(bpc2, ((int64_t)blockIdx.x - cta1) * bpc2, n2, rows + n1, rp, ci, len, i0, boff,
-                                  vals, x, z, y, alpha, beta, dinv, doff);
+    typed_rows<T, NP, 2, V, MODE>(bpc2, ((int64_t)blockIdx.x - cta1) * bpc2, n2, rows + n1, rp, tb, i0, vals, x, z,
+                                  y, alpha, beta, dinv, doff);
 }
 
 // y = alpha * Dinv * b (block diagonal, column-major blocks)
@@ -476,7 +475,7 @@ void finish_structure(Matrix& M) {
   bool two_at_most = M.nb > 0;
   for (int64_t i = 0; i < M.nb && two_at_most; ++i) two_at_most = M.h_len[i] == M.Np || M.h_len[i] == 2 * M.Np;
   const bool np_ok = M.Np == 1 || M.Np == 4 || M.Np == 10 || M.Np == 20;
-  if (!M.uniform && two_at_most && np_ok && M.Np % M.V == 0) {
+  if (!M.uniform && two_at_most && np_ok && M.Np % M.V == 0 && M.N < (int64_t)INT32_MAX) {
     std::vector<int32_t> g;
     g.reserve(M.nb);
     for (int64_t i = 0; i < M.nb; ++i)
@@ -487,6 +486,15 @@ void finish_structure(Matrix& M) {
     M.grp_n2 = (int64_t)g.size() - M.grp_n1;
     M.grp_rows.alloc(g.size());
     BSGPU_CUDA(cudaMemcpy(M.grp_rows.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
+    std::vector<TypedBlock> tb(std::max<int64_t>(M.nnzb, 1));
+    for (int64_t k = 0; k < M.nnzb; ++k) {
+      const int32_t j = M.h_ci[k];
+      tb[k].boff = boff[k];
+      tb[k].xoff = (int)M.h_i0[j];
+      tb[k].nsp = M.h_len[j] / M.Np;
+    }
+    M.tblk.alloc(tb.size());
+    BSGPU_CUDA(cudaMemcpy(M.tblk.p, tb.data(), tb.size() * sizeof(TypedBlock), cudaMemcpyHostToDevice));
     M.typed = true;
   }
   M.row2blk.alloc(std::max<int64_t>(M.N, 1));
@@ -565,8 +573,8 @@ void launch_typed(const Matrix& A, const T* vals, const T* x, const T* z, T* y, 
   const int64_t cta1 = (A.grp_n1 + bpc1 - 1) / bpc1, cta2 = (A.grp_n2 + bpc2 - 1) / bpc2;
   if (cta1 + cta2 == 0) return;
   spmv_typed_kernel<T, NP, V, MODE><<<(unsigned)(cta1 + cta2), threads, 0, st>>>(
-      A.rp.p, A.ci.p, A.len.p, A.i0.p, A.boff.p, A.grp_rows.p, A.grp_n1, A.grp_n2, cta1, vals, x, z, y, alpha, beta,
-      dinv, doff, active);
+      A.rp.p, A.tblk.p, A.i0.p, A.grp_rows.p, A.grp_n1, A.grp_n2, cta1, vals, x, z, y, alpha, beta, dinv, doff,
+      active);
   BSGPU_CHECK_LAUNCH();
 }
 

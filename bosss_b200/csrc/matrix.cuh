@@ -16,6 +16,14 @@
 
 namespace bsgpu {
 
+// Per-block metadata of the species-count kernels, one 16-byte load per block: the block's value offset, the
+// offset of its column's entries in x and the column's species count.
+struct alignas(16) TypedBlock {
+  long long boff;
+  int xoff;
+  int nsp;
+};
+
 struct Matrix {
   int64_t nb = 0, N = 0, nnzb = 0;
   int Np = 0;            // modes per species
@@ -37,6 +45,7 @@ struct Matrix {
   // kernel with per-row lookups serves the matrix).
   bool typed = false;
   DBuf<int32_t> grp_rows;
+  DBuf<TypedBlock> tblk;  // [nnzb]
   int64_t grp_n1 = 0, grp_n2 = 0;
   // Launch shape of the uniform and species-count kernels: threads per CTA (whole block rows each) for the plain
   // product (cta[0]) and the fused block-Jacobi update (cta[1]); 256 unless the autotuner picked otherwise.
