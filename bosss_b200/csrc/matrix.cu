@@ -829,9 +829,12 @@ bool cg_direction_impl(const Matrix& A, const T* vals, const T* z, const T* pold
   check_aligned(z, 16, "z");
   check_aligned(pold, 16, "p");
   if (!red.grid) red.init();
+  // one tile of block rows per CTA where the scratch allows: the single product's partial sums may use all
+  // kMaxDots * grid slots of the reduction scratch
+  const int64_t grid_cap = (int64_t)kMaxDots * red.grid;
   constexpr int VW = sizeof(T) == 8 ? 2 : 4;
 #define BSGPU_CGD(NP, VV)                                                                                       \
-  cg_direction_kernel<T, NP, VV><<<(unsigned)std::min<int64_t>((A.nb + 256 / NP - 1) / (256 / NP), red.grid),     \
+  cg_direction_kernel<T, NP, VV><<<(unsigned)std::min<int64_t>((A.nb + 256 / NP - 1) / (256 / NP), grid_cap),      \
                                    256, 0, st>>>(A.rp.p, A.ci.p, vals, z, pold, pnew, q, beta, A.nb, active,      \
                                                  red.partial.p, red.ticket.p, sigma)
   switch (A.Np) {
