@@ -7,7 +7,6 @@
 
 #include "ldst.cuh"
 #include "matrix.cuh"
-#include "reduce.cuh"
 
 namespace bsgpu {
 
@@ -170,62 +169,6 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
   }
 }
 
-// CG search direction and its image in one pass (uniform blocks): p_new = z + beta p_old, q = A p_new, and
-// sigma = p_new . q as a grid reduction.  The gathered entries of p_new are formed on the fly from z and p_old, so
-// p_old stays readable by every CTA while each CTA writes its own rows of p_new (a second buffer), and the separate
-// direction update and dot product launches of the textbook iteration disappear.  The arithmetic of p_new and of
-// the row products is that of xpby followed by the uniform SpMV.
-template <typename T, int NP, int V>
-__global__ void __launch_bounds__(256) cg_direction_kernel(
-    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const T* __restrict__ vals,
-    const T* __restrict__ z, const T* __restrict__ pold, T* __restrict__ pnew, T* __restrict__ q,
-    const double* __restrict__ beta_p, int64_t nb, const int* __restrict__ active, double* __restrict__ partial,
-    unsigned int* __restrict__ ticket, double* __restrict__ sigma) {
-  static_assert(NP % V == 0, "chunk width must divide the block size");
-  if (*active == 0) return;
-  constexpr int BPC = 256 / NP;
-  const double beta = *beta_p;
-  const int t = threadIdx.x;
-  const int lb = t / NP;
-  const int r = t - lb * NP;
-  const uint64_t pol = policy_evict_first();
-  double acc[1] = {0.0};
-  for (int64_t tile = blockIdx.x; tile * BPC < nb; tile += gridDim.x) {
-    const int64_t i = tile * BPC + lb;
-    if (lb < BPC && i < nb) {
-      T a0 = 0, a1 = 0;
-      const int64_t k0 = rp[i], k1 = rp[i + 1];
-      for (int64_t k = k0; k < k1; ++k) {
-        const int64_t j = ci[k];
-        const T* vb = vals + k * (NP * NP) + r * V;
-        const T* zb = z + j * NP;
-        const T* pb = pold + j * NP;
-#pragma unroll
-        for (int c = 0; c < NP / V; ++c) {
-          Vec<T, V> a = ldv_stream<T, V>(vb + c * (NP * V), pol);
-          Vec<T, V> zv = ldv_cached<T, V>(zb + c * V);
-          Vec<T, V> pv = ldv_cached<T, V>(pb + c * V);
-#pragma unroll
-          for (int e = 0; e < V; ++e) {
-            const T xv = (T)((double)zv.a[e] + beta * (double)pv.a[e]);
-            if ((c * V + e) & 1)
-              a1 = fma(a.a[e], xv, a1);
-            else
-              a0 = fma(a.a[e], xv, a0);
-          }
-        }
-      }
-      const int64_t g = i * NP + r;
-      const T qv = a0 + a1;
-      const T pn = (T)((double)z[g] + beta * (double)pold[g]);
-      pnew[g] = pn;
-      q[g] = qv;
-      acc[0] = fma((double)pn, (double)qv, acc[0]);
-    }
-  }
-  gridred::finish_dots<1>(acc, 1, partial, ticket, sigma, 0);
-}
-
 // General block sizes (XDG: 1..n species per block).  CTA b owns DOF rows cta_row0[b] .. cta_row0[b+1]-1,
 // which are whole block rows (packed on the host).
 template <typename T, int V, int MODE>
@@ -300,8 +243,9 @@ __global__ void __launch_bounds__(256) spmv_general_kernel(
 // so no chunk straddles a species boundary and there is no scalar tail).
 template <typename T, int NP, int NS, int V, int MODE>
 __device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, const int32_t* __restrict__ rows,
-                                           const int64_t* __restrict__ rp, const TypedBlock* __restrict__ tb,
-                                           const int64_t* __restrict__ i0, const T* __restrict__ vals,
+                                           const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                           const int32_t* __restrict__ len, const int64_t* __restrict__ i0,
+                                           const int64_t* __restrict__ boff, const T* __restrict__ vals,
                                            const T* __restrict__ x, const T* __restrict__ z, T* __restrict__ y,
                                            T alpha, T beta, const T* __restrict__ dinv,
                                            const int64_t* __restrict__ doff) {
@@ -318,10 +262,10 @@ __device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, c
   if (valid) {
     const int64_t k0 = rp[i], k1 = rp[i + 1];
     for (int64_t k = k0; k < k1; ++k) {
-      const TypedBlock m = tb[k];
-      const int sj = m.nsp;
-      const T* vb = vals + m.boff + r * V;
-      const T* xb = x + m.xoff;
+      const int64_t j = ci[k];
+      const int sj = len[j] / NP;
+      const T* vb = vals + boff[k] + r * V;
+      const T* xb = x + i0[j];
       for (int sp = 0; sp < sj; ++sp) {
 #pragma unroll
         for (int c = 0; c < NP / V; ++c) {
@@ -368,19 +312,19 @@ __device__ __forceinline__ void typed_rows(int BPC, int64_t b0, int64_t nrows, c
 // One launch for both species counts: CTAs [0, cta1) take the one-species rows, the rest the two-species rows.
 template <typename T, int NP, int V, int MODE>
 __global__ void __launch_bounds__(256) spmv_typed_kernel(
-    const int64_t* __restrict__ rp, const TypedBlock* __restrict__ tb, const int64_t* __restrict__ i0,
-    const int32_t* __restrict__ rows,
+    const int64_t* __restrict__ rp, const int32_t* __restrict__ ci, const int32_t* __restrict__ len,
+    const int64_t* __restrict__ i0, const int64_t* __restrict__ boff, const int32_t* __restrict__ rows,
     int64_t n1, int64_t n2, int64_t cta1, const T* __restrict__ vals, const T* __restrict__ x,
     const T* __restrict__ z, T* __restrict__ y, T alpha, T beta, const T* __restrict__ dinv,
     const int64_t* __restrict__ doff, const int* __restrict__ active) {
   if (active != nullptr && *active == 0) return;
   const int bpc1 = blockDim.x / NP, bpc2 = blockDim.x / (2 * NP);
   if ((int64_t)blockIdx.x < cta1)
-    typed_rows<T, NP, 1, V, MODE>(bpc1, (int64_t)blockIdx.x * bpc1, n1, rows, rp, tb, i0, vals, x, z, y, alpha,
-                                  beta, dinv, doff);
+    typed_rows<T, NP, 1, V, MODE>(bpc1, (int64_t)blockIdx.x * bpc1, n1, rows, rp, ci, len, i0, boff, vals, x, z, y,
+                                  alpha, beta, dinv, doff);
   else
-    typed_rows<T, NP, 2, V, MODE>(bpc2, ((int64_t)blockIdx.x - cta1) * bpc2, n2, rows + n1, rp, tb, i0, vals, x, z,
-                                  y, alpha, beta, dinv, doff);
+    typed_rows<T, NP, 2, V, MODE>(bpc2, ((int64_t)blockIdx.x - cta1) * bpc2, n2, rows + n1, rp, ci, len, i0, boff,
+                                  vals, x, z, y, alpha, beta, dinv, doff);
 }
 
 // y = alpha * Dinv * b (block diagonal, column-major blocks)
@@ -475,7 +419,7 @@ void finish_structure(Matrix& M) {
   bool two_at_most = M.nb > 0;
   for (int64_t i = 0; i < M.nb && two_at_most; ++i) two_at_most = M.h_len[i] == M.Np || M.h_len[i] == 2 * M.Np;
   const bool np_ok = M.Np == 1 || M.Np == 4 || M.Np == 10 || M.Np == 20;
-  if (!M.uniform && two_at_most && np_ok && M.Np % M.V == 0 && M.N < (int64_t)INT32_MAX) {
+  if (!M.uniform && two_at_most && np_ok && M.Np % M.V == 0) {
     std::vector<int32_t> g;
     g.reserve(M.nb);
     for (int64_t i = 0; i < M.nb; ++i)
@@ -486,15 +430,6 @@ void finish_structure(Matrix& M) {
     M.grp_n2 = (int64_t)g.size() - M.grp_n1;
     M.grp_rows.alloc(g.size());
     BSGPU_CUDA(cudaMemcpy(M.grp_rows.p, g.data(), g.size() * 4, cudaMemcpyHostToDevice));
-    std::vector<TypedBlock> tb(std::max<int64_t>(M.nnzb, 1));
-    for (int64_t k = 0; k < M.nnzb; ++k) {
-      const int32_t j = M.h_ci[k];
-      tb[k].boff = boff[k];
-      tb[k].xoff = (int)M.h_i0[j];
-      tb[k].nsp = M.h_len[j] / M.Np;
-    }
-    M.tblk.alloc(tb.size());
-    BSGPU_CUDA(cudaMemcpy(M.tblk.p, tb.data(), tb.size() * sizeof(TypedBlock), cudaMemcpyHostToDevice));
     M.typed = true;
   }
   M.row2blk.alloc(std::max<int64_t>(M.N, 1));
@@ -573,8 +508,8 @@ void launch_typed(const Matrix& A, const T* vals, const T* x, const T* z, T* y, 
   const int64_t cta1 = (A.grp_n1 + bpc1 - 1) / bpc1, cta2 = (A.grp_n2 + bpc2 - 1) / bpc2;
   if (cta1 + cta2 == 0) return;
   spmv_typed_kernel<T, NP, V, MODE><<<(unsigned)(cta1 + cta2), threads, 0, st>>>(
-      A.rp.p, A.tblk.p, A.i0.p, A.grp_rows.p, A.grp_n1, A.grp_n2, cta1, vals, x, z, y, alpha, beta, dinv, doff,
-      active);
+      A.rp.p, A.ci.p, A.len.p, A.i0.p, A.boff.p, A.grp_rows.p, A.grp_n1, A.grp_n2, cta1, vals, x, z, y, alpha, beta,
+      dinv, doff, active);
   BSGPU_CHECK_LAUNCH();
 }
 
@@ -819,47 +754,6 @@ void spmv(const Matrix& A, float alpha, const float* x, float beta, const float*
   check_aligned(x, 16, "x");
   if (A.half) return dispatch_half<0>(A, x, z, y, alpha, beta, nullptr, st, active);
   dispatch<float, 0>(A, A.v32.p, x, z, y, alpha, beta, nullptr, nullptr, st, active);
-}
-
-namespace {
-template <typename T>
-bool cg_direction_impl(const Matrix& A, const T* vals, const T* z, const T* pold, T* pnew, T* q, const double* beta,
-                       double* sigma, ReduceScratch& red, const int* active, cudaStream_t st) {
-  if (!specialised(A) || A.half || A.nb == 0) return false;
-  check_aligned(z, 16, "z");
-  check_aligned(pold, 16, "p");
-  if (!red.grid) red.init();
-  // one tile of block rows per CTA where the scratch allows: the single product's partial sums may use all
-  // kMaxDots * grid slots of the reduction scratch
-  const int64_t grid_cap = (int64_t)kMaxDots * red.grid;
-  constexpr int VW = sizeof(T) == 8 ? 2 : 4;
-#define BSGPU_CGD(NP, VV)                                                                                       \
-  cg_direction_kernel<T, NP, VV><<<(unsigned)std::min<int64_t>((A.nb + 256 / NP - 1) / (256 / NP), grid_cap),      \
-                                   256, 0, st>>>(A.rp.p, A.ci.p, vals, z, pold, pnew, q, beta, A.nb, active,      \
-                                                 red.partial.p, red.ticket.p, sigma)
-  switch (A.Np) {
-    case 20: BSGPU_CGD(20, VW); break;
-    case 4: BSGPU_CGD(4, VW); break;
-    case 10: BSGPU_CGD(10, 2); break;
-    default: BSGPU_CGD(6, 2); break;
-  }
-#undef BSGPU_CGD
-  BSGPU_CHECK_LAUNCH();
-  return true;
-}
-}  // namespace
-
-bool cg_direction_supported(const Matrix& A) { return specialised(A) && !A.half && A.nb > 0; }
-
-bool cg_direction(const Matrix& A, const double* z, const double* pold, double* pnew, double* q, const double* beta,
-                  double* sigma, ReduceScratch& red, const int* active, cudaStream_t st) {
-  require(!A.single, "FP64 CG direction on an FP32 matrix");
-  return cg_direction_impl<double>(A, A.v64.p, z, pold, pnew, q, beta, sigma, red, active, st);
-}
-bool cg_direction(const Matrix& A, const float* z, const float* pold, float* pnew, float* q, const double* beta,
-                  double* sigma, ReduceScratch& red, const int* active, cudaStream_t st) {
-  require(A.single, "FP32 CG direction on an FP64 matrix");
-  return cg_direction_impl<float>(A, A.v32.p, z, pold, pnew, q, beta, sigma, red, active, st);
 }
 
 namespace {

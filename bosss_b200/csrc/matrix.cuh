@@ -11,18 +11,9 @@
 #pragma once
 #include <cuda_fp16.h>
 
-#include "blas1.cuh"
 #include "common.cuh"
 
 namespace bsgpu {
-
-// Per-block metadata of the species-count kernels, one 16-byte load per block: the block's value offset, the
-// offset of its column's entries in x and the column's species count.
-struct alignas(16) TypedBlock {
-  long long boff;
-  int xoff;
-  int nsp;
-};
 
 struct Matrix {
   int64_t nb = 0, N = 0, nnzb = 0;
@@ -45,7 +36,6 @@ struct Matrix {
   // kernel with per-row lookups serves the matrix).
   bool typed = false;
   DBuf<int32_t> grp_rows;
-  DBuf<TypedBlock> tblk;  // [nnzb]
   int64_t grp_n1 = 0, grp_n2 = 0;
   // Launch shape of the uniform and species-count kernels: threads per CTA (whole block rows each) for the plain
   // product (cta[0]) and the fused block-Jacobi update (cta[1]); 256 unless the autotuner picked otherwise.
@@ -79,14 +69,6 @@ void spmv(const Matrix& A, double alpha, const double* x, double beta, const dou
           const int* active = nullptr);
 void spmv(const Matrix& A, float alpha, const float* x, float beta, const float* z, float* y, cudaStream_t st,
           const int* active = nullptr);
-// CG direction in one pass for uniform blocks of 4, 6, 10 or 20 (FP32/FP64 values): pnew = z + (*beta) pold,
-// q = A pnew, *sigma = pnew . q.  pnew must not alias pold.  Predicated on *active.  Returns false (nothing
-// launched) for other matrices.
-bool cg_direction(const Matrix& A, const double* z, const double* pold, double* pnew, double* q, const double* beta,
-                  double* sigma, ReduceScratch& red, const int* active, cudaStream_t st);
-bool cg_direction(const Matrix& A, const float* z, const float* pold, float* pnew, float* q, const double* beta,
-                  double* sigma, ReduceScratch& red, const int* active, cudaStream_t st);
-bool cg_direction_supported(const Matrix& A);
 // Block-Jacobi update fused into the SpMV: xo = x + omega * Dinv * (b - A*x).  Dinv: per block row, column-major.
 void bj_update(const Matrix& A, const double* dinv, double omega, const double* x, const double* b, double* xo,
                cudaStream_t st, const int* active = nullptr);

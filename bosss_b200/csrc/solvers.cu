@@ -606,7 +606,6 @@ __global__ void pcg_init_kernel(double* s, int* active) {
   s[0] = s[2];  // rz
   s[4] = s[3];  // rr0
   s[5] = 0.0;
-  s[6] = 0.0;   // beta of the first direction (p = z)
   *active = 1;
 }
 
@@ -615,12 +614,10 @@ struct PCGT : Solver<T> {
   const Matrix* A;
   DBuf<T> dinv;
   DBuf<T> r, z, p, q;
-  DBuf<T> p2;        // second direction buffer of the fused iteration (directions alternate between p and p2)
-  bool dir_fused = false;  // direction, its image and p.q in one launch (cg_direction)
   double* s;
   int* active;
   Term term;
-  int batch = 8;     // even: an iteration pair returns the direction to p
+  int batch = 8;
   bool precond;
   bool use_graph = true;
   cudaGraphExec_t graph_exec = nullptr;
@@ -646,16 +643,6 @@ struct PCGT : Solver<T> {
       c.check_flag(err, "PCG: singular diagonal block");
     }
     c.tune(*A, 0);
-    dir_fused = precond && A->uniform && (A->Np == 4 || A->Np == 6 || A->Np == 10 || A->Np == 20) &&
-                cg_direction_supported(*A);
-    if (dir_fused) p2.alloc(N);
-  }
-  // one fused iteration: direction pnew from pold (and its image q, p.q), then the update of x, r, z, r.z, r.r, beta
-  // and the termination test; two launches
-  void fused_iteration(Ctx& c, T* X, const T* pold, T* pnew) {
-    cg_direction(*A, z.p, pold, pnew, q.p, s + 6, s + 1, c.red, active, c.st);
-    pcg_update(c.red, A->Np, s, active, X, pnew, q.p, r.p, z.p, dinv.p, A->nb, term.mode, term.tol, term.max_iter,
-               term.min_iter, c.st);
   }
   void apply_pc(Ctx& c, const T* in, T* out, const int* act) {
     if (precond)
@@ -695,13 +682,6 @@ struct PCGT : Solver<T> {
       const T* px[1] = {p.p};
       const T* qx[1] = {q.p};
       auto batch_kernels = [&]() {
-        if (dir_fused) {
-          for (int bi = 0; bi < batch; bi += 2) {
-            fused_iteration(c, X, p.p, p2.p);
-            fused_iteration(c, X, p2.p, p.p);
-          }
-          return;
-        }
         for (int bi = 0; bi < batch; ++bi) {
           spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, st, active);
           dots(c.red, 1, px, qx, N, s + 1, 0, st, active);
@@ -797,13 +777,7 @@ struct PCGT : Solver<T> {
     const int body = c.new_body((this->trace >= 0 ? c.trace[this->trace].name + ": " : std::string()) + "CG iteration");
     cond_set(h, active, nullptr, nullptr, 0, c.exec_of(body), c.st);
     c.cond_begin(h, cudaGraphCondTypeWhile, body);
-    if (dir_fused) {
-      // two iterations per body, so that the direction returns to p (the second is a no-op once converged)
-      fused_iteration(c, X, p.p, p2.p);
-      fused_iteration(c, X, p2.p, p.p);
-    } else {
-      iteration_kernels(c, X);
-    }
+    iteration_kernels(c, X);
     cond_set(h, active, nullptr, nullptr, 0, c.exec_of(body), c.st);
     c.cond_end();
   }
