@@ -53,7 +53,11 @@ class BatchSummary:
                 "iterations_p50": float(np.percentile([r.iterations for r in self.results], 50)),
                 "iterations_max": max(r.iterations for r in self.results),
                 "all_converged": all(r.converged for r in self.results),
-                "relres_max": max(r.relres for r in self.results)}
+                "relres_max": max(r.relres for r in self.results),
+                # set-up phases summed over the problems (matrix upload and layout, change of basis, solvers of
+                # every configuration with their factorisations, autotuning and graph recordings)
+                "setup_phases_s": {k: float(sum(r.info.get(k, 0.0) for r in self.results))
+                                   for k in ("matrix_s", "change_of_basis_s", "solvers_s")}}
 
 
 class BatchSolver:
@@ -82,15 +86,21 @@ class BatchSolver:
         from .solvers import BlockMsrMatrix, MultigridOperator
         t0 = time.perf_counter()
         M = BlockMsrMatrix.from_system(system)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
         op = MultigridOperator(M)
         if self.prepare is not None:
             self.prepare(op, system)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
         slv = self.make_solver(op)
         slvs = slv if isinstance(slv, dict) else {"": slv}
         B = torch.from_numpy(np.ascontiguousarray(system.rhs, np.float64)).to(self.device)
         X = {k: torch.zeros_like(B) for k in slvs}
         torch.cuda.synchronize()
-        return dict(M=M, op=op, slv=slvs, B=B, X=X, setup_s=time.perf_counter() - t0, dof=int(system.N))
+        t3 = time.perf_counter()
+        return dict(M=M, op=op, slv=slvs, B=B, X=X, setup_s=t3 - t0, dof=int(system.N),
+                    phases={"matrix_s": t1 - t0, "change_of_basis_s": t2 - t1, "solvers_s": t3 - t2})
 
     @staticmethod
     def _collect(name, wave, times, results, on_result):
@@ -101,7 +111,8 @@ class BatchSolver:
             rel = (torch.linalg.norm(r) / torch.linalg.norm(w["B"])).item()
             slv = w["slv"][name]
             res = BatchResult(index=i, dof=w["dof"], setup_s=w["setup_s"], solve_s=times[i],
-                              iterations=slv.ThisLevelIterations, converged=slv.Converged, relres=rel)
+                              iterations=slv.ThisLevelIterations, converged=slv.Converged, relres=rel,
+                              info=dict(w.get("phases", {})))
             results.setdefault(name, []).append(res)
             if on_result is not None:
                 on_result(name, res, w)
