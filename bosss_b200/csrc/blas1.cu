@@ -155,9 +155,7 @@ bool pcg_update_impl(ReduceScratch& red, int NP, double* s, int* active, T* x, c
   if (nb == 0) return false;
   if (!red.grid) red.init();
   const int64_t tiles = (nb + 256 / NP - 1) / (256 / NP);
-  // one tile per CTA where the scratch allows (the two products' partial sums use kMaxDots * grid / 2 slots each):
-  // with the grid capped at red.grid the update ran at half occupancy and 0.5 of the HBM peak
-  const int grid = (int)std::min<int64_t>(tiles, (int64_t)(kMaxDots / 2) * red.grid);
+  const int grid = (int)std::min<int64_t>(tiles, red.grid);
 #define BSGPU_PCGU(N_)                                                                                          \
   pcg_update_kernel<T, N_><<<grid, 256, 0, st>>>(s, active, x, p, q, r, z, dinv, nb, red.partial.p, red.ticket.p, \
                                                  mode, tol, max_iter, min_iter)

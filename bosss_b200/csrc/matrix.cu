@@ -7,7 +7,6 @@
 
 #include "ldst.cuh"
 #include "matrix.cuh"
-#include "reduce.cuh"
 
 namespace bsgpu {
 
@@ -168,53 +167,6 @@ __global__ void __launch_bounds__(256) spmv_uniform_kernel(
       y[g] = fma(alpha, s0 + s1, x[g]);
     }
   }
-}
-
-// CG product with its dot product in one launch (uniform blocks, 256-thread CTAs, one tile of block rows each):
-// q = A p and *pq = p . q (grid reduction of the rows' p_g q_g, fixed summation order).  The row products are those
-// of the uniform kernel; only the separate dot-product launch and its second read of p and q disappear.
-template <typename T, int NP, int V>
-__global__ void __launch_bounds__(256) spmv_dot_kernel(const int64_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                       const T* __restrict__ vals, const T* __restrict__ p,
-                                                       T* __restrict__ q, int64_t nb, const int* __restrict__ active,
-                                                       double* __restrict__ partial,
-                                                       unsigned int* __restrict__ ticket, double* __restrict__ pq) {
-  static_assert(NP % V == 0, "chunk width must divide the block size");
-  if (*active == 0) return;
-  constexpr int BPC = 256 / NP;
-  const int t = threadIdx.x;
-  const int lb = t / NP;
-  const int r = t - lb * NP;
-  const int64_t i = (int64_t)blockIdx.x * BPC + lb;
-  const bool valid = (lb < BPC) && (i < nb);
-  const uint64_t pol = policy_evict_first();
-  double acc[1] = {0.0};
-  if (valid) {
-    T a0 = 0, a1 = 0;
-    const int64_t k0 = rp[i], k1 = rp[i + 1];
-    for (int64_t k = k0; k < k1; ++k) {
-      const int64_t j = ci[k];
-      const T* vb = vals + k * (NP * NP) + r * V;
-      const T* xb = p + j * NP;
-#pragma unroll
-      for (int c = 0; c < NP / V; ++c) {
-        Vec<T, V> a = ldv_stream<T, V>(vb + c * (NP * V), pol);
-        Vec<T, V> xv = ldv_cached<T, V>(xb + c * V);
-#pragma unroll
-        for (int e = 0; e < V; ++e) {
-          if ((c * V + e) & 1)
-            a1 = fma(a.a[e], xv.a[e], a1);
-          else
-            a0 = fma(a.a[e], xv.a[e], a0);
-        }
-      }
-    }
-    const int64_t g = i * NP + r;
-    const T qv = a0 + a1;
-    q[g] = qv;
-    acc[0] = (double)p[g] * (double)qv;
-  }
-  gridred::finish_dots<1>(acc, 1, partial, ticket, pq, 0);
 }
 
 // General block sizes (XDG: 1..n species per block).  CTA b owns DOF rows cta_row0[b] .. cta_row0[b+1]-1,
@@ -802,44 +754,6 @@ void spmv(const Matrix& A, float alpha, const float* x, float beta, const float*
   check_aligned(x, 16, "x");
   if (A.half) return dispatch_half<0>(A, x, z, y, alpha, beta, nullptr, st, active);
   dispatch<float, 0>(A, A.v32.p, x, z, y, alpha, beta, nullptr, nullptr, st, active);
-}
-
-namespace {
-template <typename T>
-bool spmv_dot_impl(const Matrix& A, const T* vals, const T* p, T* q, double* pq, ReduceScratch& red,
-                   const int* active, cudaStream_t st) {
-  if (!specialised(A) || A.half || A.nb == 0) return false;
-  if (!red.grid) red.init();
-  const int NP = A.Np;
-  const int64_t grid = (A.nb + 256 / NP - 1) / (256 / NP);
-  // one partial sum per CTA: the single product may use all kMaxDots * grid slots of the scratch
-  if (grid > (int64_t)kMaxDots * red.grid) return false;
-  check_aligned(p, 16, "p");
-  constexpr int VW = sizeof(T) == 8 ? 2 : 4;
-#define BSGPU_SPD(NP_, VV)                                                                                   \
-  spmv_dot_kernel<T, NP_, VV><<<(unsigned)grid, 256, 0, st>>>(A.rp.p, A.ci.p, vals, p, q, A.nb, active,      \
-                                                             red.partial.p, red.ticket.p, pq)
-  switch (NP) {
-    case 20: BSGPU_SPD(20, VW); break;
-    case 4: BSGPU_SPD(4, VW); break;
-    case 10: BSGPU_SPD(10, 2); break;
-    default: BSGPU_SPD(6, 2); break;
-  }
-#undef BSGPU_SPD
-  BSGPU_CHECK_LAUNCH();
-  return true;
-}
-}  // namespace
-
-bool spmv_dot(const Matrix& A, const double* p, double* q, double* pq, ReduceScratch& red, const int* active,
-              cudaStream_t st) {
-  require(!A.single, "FP64 product on an FP32 matrix");
-  return spmv_dot_impl<double>(A, A.v64.p, p, q, pq, red, active, st);
-}
-bool spmv_dot(const Matrix& A, const float* p, float* q, double* pq, ReduceScratch& red, const int* active,
-              cudaStream_t st) {
-  require(A.single, "FP32 product on an FP64 matrix");
-  return spmv_dot_impl<float>(A, A.v32.p, p, q, pq, red, active, st);
 }
 
 namespace {

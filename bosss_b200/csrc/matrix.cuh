@@ -11,7 +11,6 @@
 #pragma once
 #include <cuda_fp16.h>
 
-#include "blas1.cuh"
 #include "common.cuh"
 
 namespace bsgpu {
@@ -70,12 +69,6 @@ void spmv(const Matrix& A, double alpha, const double* x, double beta, const dou
           const int* active = nullptr);
 void spmv(const Matrix& A, float alpha, const float* x, float beta, const float* z, float* y, cudaStream_t st,
           const int* active = nullptr);
-// CG product and its dot product in one launch for uniform blocks of 4, 6, 10 or 20 (FP32/FP64 values): q = A p,
-// *pq = p . q.  Predicated on *active.  Returns false (nothing launched) for other matrices.
-bool spmv_dot(const Matrix& A, const double* p, double* q, double* pq, ReduceScratch& red, const int* active,
-              cudaStream_t st);
-bool spmv_dot(const Matrix& A, const float* p, float* q, double* pq, ReduceScratch& red, const int* active,
-              cudaStream_t st);
 // Block-Jacobi update fused into the SpMV: xo = x + omega * Dinv * (b - A*x).  Dinv: per block row, column-major.
 void bj_update(const Matrix& A, const double* dinv, double omega, const double* x, const double* b, double* xo,
                cudaStream_t st, const int* active = nullptr);

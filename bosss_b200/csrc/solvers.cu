@@ -683,10 +683,8 @@ struct PCGT : Solver<T> {
       const T* qx[1] = {q.p};
       auto batch_kernels = [&]() {
         for (int bi = 0; bi < batch; ++bi) {
-          if (!spmv_dot(*A, p.p, q.p, s + 1, c.red, active, st)) {
-            spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, st, active);
-            dots(c.red, 1, px, qx, N, s + 1, 0, st, active);
-          }
+          spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, st, active);
+          dots(c.red, 1, px, qx, N, s + 1, 0, st, active);
           if (fused) {
             // alpha, x and r updates, z = Dinv r, r.z, r.r and the beta / termination step in one launch
             pcg_update(c.red, A->Np, s, active, X, p.p, q.p, r.p, z.p, dinv.p, A->nb, term.mode, term.tol,
@@ -790,10 +788,8 @@ struct PCGT : Solver<T> {
     const bool fused = precond && A->uniform && A->nb > 0 && (A->Np == 4 || A->Np == 6 || A->Np == 10 || A->Np == 20);
     const T* px[1] = {p.p};
     const T* qx[1] = {q.p};
-    if (!spmv_dot(*A, p.p, q.p, s + 1, c.red, active, c.st)) {
-      spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, c.st, active);
-      dots(c.red, 1, px, qx, N, s + 1, 0, c.st, active);
-    }
+    spmv(*A, T(1), p.p, T(0), (const T*)nullptr, q.p, c.st, active);
+    dots(c.red, 1, px, qx, N, s + 1, 0, c.st, active);
     if (fused) {
       pcg_update(c.red, A->Np, s, active, X, p.p, q.p, r.p, z.p, dinv.p, A->nb, term.mode, term.tol, term.max_iter,
                  term.min_iter, c.st);
