@@ -155,7 +155,8 @@ bool pcg_update_impl(ReduceScratch& red, int NP, double* s, int* active, T* x, c
   if (nb == 0) return false;
   if (!red.grid) red.init();
   const int64_t tiles = (nb + 256 / NP - 1) / (256 / NP);
-  const int grid = (int)std::min<int64_t>(tiles, red.grid);
+  // one full wave (8 CTAs of 256 threads per SM at 32 registers); more CTAs serialise on the reduction's ticket
+  const int grid = (int)std::min<int64_t>(tiles, 2 * (int64_t)red.grid);
 #define BSGPU_PCGU(N_)                                                                                          \
   pcg_update_kernel<T, N_><<<grid, 256, 0, st>>>(s, active, x, p, q, r, z, dinv, nb, red.partial.p, red.ticket.p, \
                                                  mode, tol, max_iter, min_iter)
