@@ -27,3 +27,15 @@ def test_other_workloads_reference_arm_is_explicit():
     assert out.returncode == 0
     d = json.loads(out.stdout.strip().splitlines()[-1])
     assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_learned_training_solve_count():
+    """The learned variant collects 200 training residuals: enough seeded solves of the fast form's iteration
+    count, at least 2 and at most 25."""
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.learned_rhs_count(9) == 24 and bench.learned_rhs_count(41) == 6
+    assert bench.learned_rhs_count(1) == 25 and bench.learned_rhs_count(500) == 2
+    for it in (1, 5, 9, 17, 41, 120):
+        n = bench.learned_rhs_count(it)
+        assert n * it >= 200 or n == 25
