@@ -37,6 +37,7 @@ struct bsgpu_solver_s {
   cudaGraphExec_t rec_exec = nullptr;
   long long rec_top = 0;  // kernels at the top level of the recording
   int rec_key = -1;
+  int device = 0;         // the device the handle's memory lives on
   ~bsgpu_solver_s() {
     if (rec_exec) cudaGraphExecDestroy(rec_exec);
   }
@@ -487,6 +488,7 @@ BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgp
     h->X.alloc(N); h->B.alloc(N); h->Xt.alloc(N); h->Bt.alloc(N);
     BSGPU_CUDA(cudaEventCreate(&h->e0));
     BSGPU_CUDA(cudaEventCreate(&h->e1));
+    BSGPU_CUDA(cudaGetDevice(&h->device));
     ensure_recorded(h.get());  // cfg.graph == 2: the whole solve is recorded at set-up
     *s = h.release();
   });
@@ -495,11 +497,16 @@ BSGPU_API int bsgpu_solver_create(bsgpu_solver_t* s, bsgpu_mgop_t op, const bsgp
 BSGPU_API int bsgpu_batch_create(bsgpu_batch_t* b, const bsgpu_solver_t* solvers, int32_t n) {
   return guarded([&] {
     require(b && solvers && n >= 1, "null argument or empty batch");
+    require(solvers[0] != nullptr, "null solver handle in the batch");
+    int cur = 0;
+    BSGPU_CUDA(cudaGetDevice(&cur));
+    require(cur == solvers[0]->device, "the current device must be the batch members' device (bsgpu_set_device)");
     auto h = std::make_unique<bsgpu_batch_s>();
     for (int32_t i = 0; i < n; ++i) {
       bsgpu_solver_s* s = solvers[i];
       require(s != nullptr, "null solver handle in the batch");
       for (int32_t q = 0; q < i; ++q) require(solvers[q] != s, "a solver handle appears twice in the batch");
+      require(s->device == solvers[0]->device, "batch members must live on one device");
       RecordedSolve* r = recorded_form(*s->tree);
       require(r != nullptr, "batch members must be FlexGMRES solvers created with graph = 2", BSGPU_ERR_UNSUPPORTED);
       r->prepare(*s->tree->ctx);
@@ -565,8 +572,12 @@ BSGPU_API int bsgpu_batch_solve_device(bsgpu_batch_t b, double* const* X, const 
   return guarded([&] {
     require(b && X && B, "null argument");
     const int n = (int)b->s.size();
+    int cur = 0;
+    BSGPU_CUDA(cudaGetDevice(&cur));
+    require(cur == b->s[0]->device, "the current device must be the batch members' device (bsgpu_set_device)");
     for (int i = 0; i < n; ++i) {
       require(X[i] && B[i], "null vector in the batch");
+      require((const double*)X[i] != B[i], "a batch member's X and B must be different vectors");
       require(recorded_form(*b->s[i]->tree)->key() == b->keys[i],
               "a batch member's learned stage was switched after the batch was recorded; create the batch again");
     }

@@ -214,3 +214,30 @@ def test_batch_solver_one_graph_waves(cuda):
         xd = O.direct_solve(s)
         for name in ("one_graph", "threads"):
             assert np.linalg.norm(sols[(name, i)] - xd) <= SOL_TOL * np.linalg.norm(xd)
+
+
+def test_batch_with_learned_stage_in_one_graph(cuda):
+    """Uniform systems, each with its trained learned stage as FlexGMRES's second preconditioner (IF nodes of the
+    round-robin inside every branch), solved from one graph launch: solutions against the direct solves.  A member
+    whose X and B are the same vector is rejected."""
+    import torch
+    systems = [A.poisson_3d(n, 2, seed=i) for i, n in enumerate((5, 6, 4))]
+    slvs = []
+    for s in systems:
+        op = MultigridOperator(BlockMsrMatrix.from_system(s))
+        op.SetCellGraph(s.grid.face_neighbours())
+        slv = _solver(op, "solve", True, learned="fgmres", DegreeHierarchy=(10, 4, 1), CoarseTolerance=0.1,
+                      CoarseMaxIterations=60, NoOfPostSmootherSweeps=2)
+        slv.TrainLearned(n_rhs=2, steps=30, seed=1)
+        slvs.append(slv)
+    Bs = [torch.from_numpy(s.rhs).cuda() for s in systems]
+    Xs = [torch.zeros_like(b) for b in Bs]
+    gb = GpuBatch(slvs)
+    gb.Solve(Xs, Bs)
+    for slv, s, X in zip(slvs, systems, Xs):
+        assert slv.Converged
+        xd = O.direct_solve(s)
+        assert np.linalg.norm(X.cpu().numpy() - xd) <= SOL_TOL * np.linalg.norm(xd)
+    with pytest.raises(nat.BsgpuError):
+        gb.Solve([Bs[0]] + Xs[1:], Bs)
+    gb.Dispose()
