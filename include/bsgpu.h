@@ -257,8 +257,10 @@ BSGPU_API int bsgpu_solver_get_trace(bsgpu_solver_t s, char* buf, size_t len);
  * i's buffers, runs every member concurrently from one graph launch, writes the solutions to X[i] and returns when
  * all are done.  stats (n entries, may be NULL): per member as bsgpu_solver_solve_device, with seconds = device time
  * from the launch to the end of that member's branch (its latency inside the batch).  The member handles must not
- * be used elsewhere while a batch solve runs; a batch whose member had its learned stage switched since create is
- * rejected (create it again).  Errors a member's solve records are raised after all results were written. */
+ * be used elsewhere while a batch solve runs, and the batch must be destroyed before its members (its graph uses
+ * their device memory); a batch whose member had its learned stage switched since create is rejected (create it
+ * again).  All members live on the current device.  Errors a member's solve records are raised after all results
+ * were written. */
 typedef struct bsgpu_batch_s* bsgpu_batch_t;
 BSGPU_API int bsgpu_batch_create(bsgpu_batch_t* b, const bsgpu_solver_t* solvers, int32_t n);
 BSGPU_API int bsgpu_batch_solve_device(bsgpu_batch_t b, double* const* X, const double* const* B,
