@@ -541,7 +541,7 @@ void hist_dots_impl(HistScratch& s, const T* const* hist, const int* k, const T*
                     double* self, cudaStream_t st) {
   require(s.chunks > 0, "history multi-dot: scratch not initialised");
   const int W = 16 / (int)sizeof(T);
-  const int G = (int)std::min<int64_t>(std::max<int64_t>(1, (n / W + kThreads - 1) / kThreads), s.grid);
+  const int G = std::min(grid_for(std::max<int64_t>(n / W, 1)), s.grid);
   require((reinterpret_cast<uintptr_t>(m) & 15) == 0, "history multi-dot: unaligned vector");
   hist_dots_kernel<T><<<dim3(G, s.chunks), kThreads, 0, st>>>(hist, k, s.chunks * kChunk > s.slots ? s.slots : s.chunks * kChunk,
                                                                 m, n, beta, self, s.partial.p, s.ticket.p);
@@ -579,7 +579,7 @@ void HistScratch::init(int cap) {
   require(cap >= 1 && cap <= kHistMax, "history length must be in 1..128");
   slots = cap;
   chunks = (cap + kChunk - 1) / kChunk;
-  grid = num_sms() * 3;  // one wave per chunk at 3 CTAs of 256 threads per SM (80 registers per thread)
+  grid = num_sms() * 2;
   partial.alloc((size_t)chunks * kProducts * grid);
   ticket.alloc(chunks);
   BSGPU_CUDA(cudaMemset(ticket.p, 0, chunks * sizeof(unsigned int)));
