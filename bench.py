@@ -281,8 +281,13 @@ def run_ours(args):
     from bosss_b200.solvers import BlockMsrMatrix, FGMRESConfig, MultigridOperator, PmgConfig
     nat.check(nat.lib().bsgpu_set_device(local))
 
+    t0 = time.perf_counter()
     s = A.poisson_3d(args.n, args.p, seed=args.seed)
+    t_host_asm = time.perf_counter() - t0
+    t0 = time.perf_counter()
     M = BlockMsrMatrix.from_system(s)
+    torch.cuda.synchronize()
+    t_upload = time.perf_counter() - t0
     t0 = time.perf_counter()
     op = MultigridOperator(M)
     torch.cuda.synchronize()
@@ -324,6 +329,20 @@ def run_ours(args):
     spmv32_ms = e0.elapsed_time(e1) / args.spmv_repeats
     nbytes32 = s.nnzb * s.Np * s.Np * 4 + s.nnzb * 4 + (s.nb + 1) * 8 + 2 * s.N * 4
     del A32, x32, y32
+    # the same operator assembled on the GPU (bsgpu_assemble_sip_cartesian) against the host assembly + upload,
+    # checked by one product with the uploaded matrix
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Mg = BlockMsrMatrix.AssembleSIP((args.n,) * 3, args.p, penalty=(args.p + 1) * (args.p + 2))
+    torch.cuda.synchronize()
+    t_gpu_asm = time.perf_counter() - t0
+    y_ref = torch.zeros_like(x)
+    M.SpMV(1.0, x, 0.0, y_ref)
+    Mg.SpMV(1.0, x, 0.0, y)
+    asm_diff = (torch.linalg.norm(y - y_ref) / torch.linalg.norm(y_ref)).item()
+    Mg.Dispose()
+    del y_ref
+    assembly = {"gpu_s": t_gpu_asm, "host_s": t_host_asm, "upload_s": t_upload, "spmv_rel_diff": asm_diff}
     if args.spmv_only:
         print(json.dumps({"spmv_fp64_gbs": spmv_gbs, "spmv_fp64_ms": spmv_avg, "bytes": nbytes,
                           "spmv_fp32_gbs": nbytes32 / (spmv32_ms * 1e-3) / 1e9, "n": args.n, "p": args.p}))
@@ -480,6 +499,7 @@ def run_ours(args):
         "spmv": {"gbs": spmv_gbs, "ms": spmv_avg, "bytes": nbytes, "repeats": args.spmv_repeats,
                  "fp32_gbs": nbytes32 / (spmv32_ms * 1e-3) / 1e9, "fp32_ms": spmv32_ms},
         "setup": {"change_of_basis_s": t_cob, "solver_setup_s": t_setup_fast, "plain_solver_setup_s": t_setup_plain},
+        "assembly": assembly,
         # change of basis + solver set-up (level matrices, FP32 copies, block inverses) + one solve
         "time_to_solution_incl_setup": t_cob + t_setup_fast + t_fast_max,
         "plain_fp64_time_to_solution_incl_setup": t_cob + t_setup_plain + plain_max,

@@ -264,6 +264,17 @@ BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, con
   });
 }
 
+BSGPU_API int bsgpu_assemble_sip_cartesian(bsgpu_matrix_t* A, int32_t D, const int32_t* shape, double lo, double hi,
+                                           int32_t p, double penalty, const double* nu, int32_t flags) {
+  return guarded([&] {
+    require(A != nullptr && shape != nullptr, "null argument");
+    require(flags == BSGPU_HOST_POINTERS || flags == BSGPU_DEVICE_POINTERS, "bad pointer flag");
+    auto h = std::make_unique<bsgpu_matrix_s>();
+    h->m.reset(assemble_sip_cartesian(D, shape, lo, hi, p, penalty, nu, flags == BSGPU_DEVICE_POINTERS));
+    *A = h.release();
+  });
+}
+
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A) {
   return guarded([&] {
     if (A && !A->borrowed) delete A;

@@ -62,6 +62,10 @@ Matrix* matrix_to_single(const Matrix& A, cudaStream_t st);
 // half the value traffic.  Marked single (it serves the FP32 kernels' entry points).
 Matrix* matrix_to_half(const Matrix& A, cudaStream_t st);
 Matrix* matrix_restrict(const Matrix& A, int keep, cudaStream_t st);
+// SIP operator of -div(nu grad u) on a uniform Cartesian grid of shape[0..D) cells over [lo, hi]^D, degree p,
+// homogeneous Dirichlet boundaries, assembled on the GPU (assembly.cu).  nu: per-cell diffusivity or null (1).
+Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi, int p, double penalty,
+                               const double* nu, bool nu_device);
 
 // y = alpha*A*x + beta*z (z may be y; z == nullptr: beta ignored).  `active`: optional device flag, the launch
 // is a no-op when *active == 0.

@@ -37,7 +37,7 @@ EXPORTS = [
     "bsgpu_solver_solve_device", "bsgpu_solver_get_history", "bsgpu_solver_set_tracing", "bsgpu_solver_get_trace",
     "bsgpu_solver_learned_info", "bsgpu_solver_learned_get_weights", "bsgpu_solver_learned_set_weights",
     "bsgpu_solver_learned_apply", "bsgpu_solver_learned_gradient",
-    "bsgpu_batch_create", "bsgpu_batch_solve_device", "bsgpu_batch_destroy",
+    "bsgpu_batch_create", "bsgpu_batch_solve_device", "bsgpu_batch_destroy", "bsgpu_assemble_sip_cartesian",
 ]
 
 
@@ -126,6 +126,7 @@ def lib() -> C.CDLL:
             "bsgpu_batch_create": [vp, vp, i32],
             "bsgpu_batch_solve_device": [vp, vp, vp, vp],
             "bsgpu_batch_destroy": [vp],
+            "bsgpu_assemble_sip_cartesian": [vp, i32, vp, dbl, dbl, i32, dbl, vp, i32],
         }
         for name, args in sig.items():
             f = getattr(L, name)

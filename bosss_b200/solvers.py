@@ -69,6 +69,49 @@ class BlockMsrMatrix:
         return M
 
     @classmethod
+    def AssembleSIP(cls, shape, p: int, penalty: Optional[float] = None, coeff=None, lo: float = 0.0,
+                    hi: float = 1.0) -> "BlockMsrMatrix":
+        """The SIP operator of -div(nu grad u) on a uniform Cartesian grid of ``shape`` cells over [lo, hi]^D,
+        degree ``p``, homogeneous Dirichlet boundaries, assembled on the GPU (bsgpu_assemble_sip_cartesian): the
+        matrix ``assembly.assemble_sip`` builds on the host (ipLaplace.cs:95-245).  ``penalty`` defaults to
+        1.3 * max((p+1)(p+D)/D, (p+1)^2); ``coeff``: per-cell diffusivity (numpy or CUDA tensor, cells x fastest)."""
+        shape = [int(n) for n in shape]
+        D = len(shape)
+        if not 1 <= D <= 3:
+            raise ValueError("shape must have 1, 2 or 3 entries")
+        if penalty is None:
+            penalty = 1.3 * max((p + 1) * (p + D) / D, (p + 1) ** 2)
+        nc = int(np.prod(shape))
+        flags, nu = nat.HOST_POINTERS, None
+        if coeff is not None:
+            if _is_device(coeff):
+                import torch
+                nu = coeff.to(torch.float64).contiguous()
+                flags = nat.DEVICE_POINTERS
+            else:
+                nu = np.ascontiguousarray(coeff, np.float64)
+            if (nu.numel() if _is_device(nu) else nu.size) != nc:
+                raise ValueError("coeff must hold one value per cell")
+        dims = (C.c_int32 * D)(*shape)
+        h = C.c_void_p()
+        nat.check(nat.lib().bsgpu_assemble_sip_cartesian(C.byref(h), D, dims, float(lo), float(hi), int(p),
+                                                         float(penalty), None if nu is None else nat.ptr(nu),
+                                                         flags))
+        M = cls(h)
+        # host copy of the block structure: block columns ascending (-z, -y, -x, self, +x, +y, +z as present)
+        ids = np.arange(nc, dtype=np.int64)
+        idx = np.unravel_index(ids, tuple(reversed(shape)))[::-1]   # per direction, x first
+        strides = [int(np.prod(shape[:d])) for d in range(D)]
+        cand = [np.where(idx[d] > 0, ids - strides[d], -1) for d in reversed(range(D))] + [ids] + \
+               [np.where(idx[d] < shape[d] - 1, ids + strides[d], -1) for d in range(D)]
+        cand = np.stack(cand, axis=1)
+        keep = cand >= 0
+        rp = np.zeros(nc + 1, np.int64)
+        np.cumsum(keep.sum(axis=1), out=rp[1:])
+        M._structure = (rp, cand[keep].astype(np.int32), None)
+        return M
+
+    @classmethod
     def from_system(cls, s) -> "BlockMsrMatrix":
         return cls.from_bsr(s.Np, s.row_ptr, s.col_idx, s.values, getattr(s, "nspc", None))
 

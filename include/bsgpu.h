@@ -75,6 +75,15 @@ BSGPU_API int bsgpu_autotune_report(char* buf, size_t len);
 BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, const int32_t* nspc,
                                   const int64_t* row_ptr, const int32_t* col_idx, const double* values,
                                   int32_t flags);
+/* SIP (symmetric interior penalty) DG operator of -div(nu grad u) on a uniform Cartesian grid of shape[0] x ... x
+ * shape[D-1] cells over [lo, hi]^D (D = 1, 2, 3; cells numbered x fastest), polynomial degree p (orthonormal
+ * Legendre products of total degree <= p, modes ordered by total degree, then lexicographically), homogeneous
+ * Dirichlet boundaries, assembled on the GPU into a new matrix handle: the matrix the host assembly of ipLaplace.cs
+ * (:95-245) produces for this grid.  Inner faces: penalty * max(cj) * max(nu) of the two cells; boundary faces:
+ * 2 * penalty * cj * nu; cj = 0.5 * (surface + boundary area) / volume (GridData_CellData.cs:681-687).  nu: per-cell
+ * diffusivity (NULL: 1), a host or device array per flags (BSGPU_HOST_POINTERS / BSGPU_DEVICE_POINTERS). */
+BSGPU_API int bsgpu_assemble_sip_cartesian(bsgpu_matrix_t* A, int32_t D, const int32_t* shape, double lo, double hi,
+                                           int32_t p, double penalty, const double* nu, int32_t flags);
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A);
 BSGPU_API int bsgpu_matrix_get_info(bsgpu_matrix_t A, int64_t* nrows, int64_t* nb, int64_t* nnzb, int32_t* Np);
 /* Copies the values back in the creation layout (row-major blocks) to a host or device buffer. */

@@ -52,3 +52,11 @@ def test_fgmres_graph_modes(graph, value):
 def test_fgmres_rejects_unknown_graph_mode():
     with pytest.raises(ValueError):
         FGMRESConfig(Graph="always")._config()
+
+
+def test_assemble_sip_rejects_bad_shapes_before_the_library():
+    from bosss_b200.solvers import BlockMsrMatrix
+    with pytest.raises(ValueError):
+        BlockMsrMatrix.AssembleSIP((2, 2, 2, 2), 1)
+    with pytest.raises(ValueError):
+        BlockMsrMatrix.AssembleSIP((3, 3), 1, coeff=[1.0, 2.0])
