@@ -204,6 +204,58 @@ __global__ void sip_assemble_kernel(SipArgs a, const double* __restrict__ tmpl, 
 
 }  // namespace
 
+std::vector<double> sip_templates(int D, int p, const double* h) {
+  require(D >= 1 && D <= 3, "D must be 1, 2 or 3");
+  require(p >= 0 && p <= 6, "p must be in 0..6");
+  const auto modes = modes_of(D, p);
+  const int Np = (int)modes.size();
+  std::vector<double> gx, gw, P, dP;
+  gauss_legendre(p + 2, gx, gw);
+  std::vector<double> S((p + 1) * (p + 1), 0.0);
+  for (size_t g = 0; g < gx.size(); ++g) {
+    legendre_all(p, gx[g], P, dP);
+    for (int m = 0; m <= p; ++m)
+      for (int n = 0; n <= p; ++n) S[m * (p + 1) + n] += gw[g] * dP[m] * dP[n];
+  }
+  std::vector<double> Pp, dPp, Pm, dPm;
+  legendre_all(p, 1.0, Pp, dPp);
+  legendre_all(p, -1.0, Pm, dPm);
+  const int NN = Np * Np;
+  std::vector<double> T((size_t)kTemplates * NN, 0.0);
+  auto expand = [&](int tid, int d, auto&& f) {
+    for (int r = 0; r < Np; ++r)
+      for (int c = 0; c < Np; ++c) {
+        bool same = true;
+        for (int e = 0; e < D; ++e)
+          if (e != d && modes[r][e] != modes[c][e]) same = false;
+        if (same) T[(size_t)tid * NN + r * Np + c] += f(modes[r][d], modes[c][d]);
+      }
+  };
+  for (int d = 0; d < D; ++d) {
+    require(h[d] > 0, "cell sizes must be positive");
+    const double hd = h[d];
+    const double s = std::sqrt(2.0 / hd);  // traces: sqrt(2/h) psi(+-1); normal derivatives: sqrt(2/h) (2/h) psi'
+    const double ds = s * 2.0 / hd;
+    auto tp = [&](int m) { return s * Pp[m]; };
+    auto dp = [&](int m) { return ds * dPp[m]; };
+    auto tm = [&](int m) { return s * Pm[m]; };
+    auto dm = [&](int m) { return ds * dPm[m]; };
+    expand(0, d, [&](int m, int n) { return 4.0 / (hd * hd) * S[m * (p + 1) + n]; });
+    const int b = 1 + 4 * d;
+    expand(b, d, [&](int m, int n) { return -0.5 * (tp(m) * dp(n) + dp(m) * tp(n)); });
+    expand(b + 1, d, [&](int m, int n) { return tp(m) * tp(n); });
+    expand(b + 2, d, [&](int m, int n) { return 0.5 * (tm(m) * dm(n) + dm(m) * tm(n)); });
+    expand(b + 3, d, [&](int m, int n) { return tm(m) * tm(n); });
+    const int ob = 1 + 4 * kMaxD + 6 * d;
+    expand(ob, d, [&](int m, int n) { return -0.5 * tp(m) * dm(n); });
+    expand(ob + 1, d, [&](int m, int n) { return 0.5 * dp(m) * tm(n); });
+    expand(ob + 2, d, [&](int m, int n) { return -tp(m) * tm(n); });
+  }
+  return T;
+}
+
+int sip_template_count() { return kTemplates; }
+
 Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi, int p, double penalty,
                                const double* nu, bool nu_device) {
   require(D >= 1 && D <= 3, "D must be 1, 2 or 3");
@@ -230,48 +282,10 @@ Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi
   const int Np = (int)modes.size();
   a.Np = Np;
   require(Np * Np <= 1024, "blocks above 32 x 32 entries are not supported");
-  // 1-D matrices: stiffness S[m][n] = int psi_m' psi_n' (exact with p + 2 Gauss points), traces at +-1
-  std::vector<double> gx, gw, P, dP;
-  gauss_legendre(p + 2, gx, gw);
-  std::vector<double> S((p + 1) * (p + 1), 0.0);
-  for (size_t g = 0; g < gx.size(); ++g) {
-    legendre_all(p, gx[g], P, dP);
-    for (int m = 0; m <= p; ++m)
-      for (int n = 0; n <= p; ++n) S[m * (p + 1) + n] += gw[g] * dP[m] * dP[n];
-  }
-  std::vector<double> Pp, dPp, Pm, dPm;
-  legendre_all(p, 1.0, Pp, dPp);
-  legendre_all(p, -1.0, Pm, dPm);
+  double hs[kMaxD] = {1.0, 1.0, 1.0};
+  for (int d = 0; d < D; ++d) hs[d] = 1.0 / a.hinv[d];
+  const std::vector<double> T = sip_templates(D, p, hs);
   const int NN = Np * Np;
-  std::vector<double> T((size_t)kTemplates * NN, 0.0);
-  auto expand = [&](int tid, int d, auto&& f) {
-    for (int r = 0; r < Np; ++r)
-      for (int c = 0; c < Np; ++c) {
-        bool same = true;
-        for (int e = 0; e < D; ++e)
-          if (e != d && modes[r][e] != modes[c][e]) same = false;
-        if (same) T[(size_t)tid * NN + r * Np + c] += f(modes[r][d], modes[c][d]);
-      }
-  };
-  for (int d = 0; d < D; ++d) {
-    const double h = 1.0 / a.hinv[d];
-    const double s = std::sqrt(2.0 / h);  // trace scaling: t = sqrt(2/h) psi(+-1), deriv: sqrt(2/h) (2/h) psi'(+-1)
-    const double ds = s * 2.0 / h;
-    auto tp = [&](int m) { return s * Pp[m]; };
-    auto dp = [&](int m) { return ds * dPp[m]; };
-    auto tm = [&](int m) { return s * Pm[m]; };
-    auto dm = [&](int m) { return ds * dPm[m]; };
-    expand(0, d, [&](int m, int n) { return 4.0 / (h * h) * S[m * (p + 1) + n]; });
-    const int b = 1 + 4 * d;
-    expand(b, d, [&](int m, int n) { return -0.5 * (tp(m) * dp(n) + dp(m) * tp(n)); });
-    expand(b + 1, d, [&](int m, int n) { return tp(m) * tp(n); });
-    expand(b + 2, d, [&](int m, int n) { return 0.5 * (tm(m) * dm(n) + dm(m) * tm(n)); });
-    expand(b + 3, d, [&](int m, int n) { return tm(m) * tm(n); });
-    const int ob = 1 + 4 * kMaxD + 6 * d;
-    expand(ob, d, [&](int m, int n) { return -0.5 * tp(m) * dm(n); });
-    expand(ob + 1, d, [&](int m, int n) { return 0.5 * dp(m) * tm(n); });
-    expand(ob + 2, d, [&](int m, int n) { return -tp(m) * tm(n); });
-  }
   // structure: block columns ascending per row (-z, -y, -x, self, +x, +y, +z as present)
   std::vector<int64_t> rp(nc + 1, 0);
   std::vector<int32_t> ci;

@@ -1,4 +1,5 @@
 // extern "C" boundary of the library (declarations and reference citations in include/bsgpu.h).
+#include <algorithm>
 #include <atomic>
 #include <cstring>
 #include <exception>
@@ -272,6 +273,18 @@ BSGPU_API int bsgpu_assemble_sip_cartesian(bsgpu_matrix_t* A, int32_t D, const i
     auto h = std::make_unique<bsgpu_matrix_s>();
     h->m.reset(assemble_sip_cartesian(D, shape, lo, hi, p, penalty, nu, flags == BSGPU_DEVICE_POINTERS));
     *A = h.release();
+  });
+}
+
+BSGPU_API int bsgpu_sip_templates(int32_t D, int32_t p, const double* h, double* out, int64_t cap, int64_t* n) {
+  return guarded([&] {
+    require(h != nullptr, "null argument");
+    const std::vector<double> T = sip_templates(D, p, h);
+    if (n) *n = (int64_t)T.size();
+    if (out) {
+      require(cap >= (int64_t)T.size(), "output buffer too small");
+      std::copy(T.begin(), T.end(), out);
+    }
   });
 }
 

@@ -66,6 +66,11 @@ Matrix* matrix_restrict(const Matrix& A, int keep, cudaStream_t st);
 // homogeneous Dirichlet boundaries, assembled on the GPU (assembly.cu).  nu: per-cell diffusivity or null (1).
 Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi, int p, double penalty,
                                const double* nu, bool nu_device);
+// the assembly's block templates for cell sizes h[0..D) (host computation, no device work): sip_template_count()
+// matrices of Np x Np, row-major (0 volume; 1 + 4d .. 4 + 4d the face terms of direction d on the +d and -d sides;
+// 13 + 6d .. 15 + 6d the off-diagonal terms of direction d)
+std::vector<double> sip_templates(int D, int p, const double* h);
+int sip_template_count();
 
 // y = alpha*A*x + beta*z (z may be y; z == nullptr: beta ignored).  `active`: optional device flag, the launch
 // is a no-op when *active == 0.

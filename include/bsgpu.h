@@ -84,6 +84,11 @@ BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, con
  * diffusivity (NULL: 1), a host or device array per flags (BSGPU_HOST_POINTERS / BSGPU_DEVICE_POINTERS). */
 BSGPU_API int bsgpu_assemble_sip_cartesian(bsgpu_matrix_t* A, int32_t D, const int32_t* shape, double lo, double hi,
                                            int32_t p, double penalty, const double* nu, int32_t flags);
+/* The block templates of that assembly for cell sizes h[0..D) (host computation, no device work): 31 row-major
+ * Np x Np matrices (0: volume term; 1+4d .. 4+4d: consistency and penalty terms of the +d and -d faces of
+ * direction d; 13+6d .. 15+6d: the off-diagonal terms of direction d).  n (may be NULL): entries; out (may be NULL
+ * to query n) holds cap entries. */
+BSGPU_API int bsgpu_sip_templates(int32_t D, int32_t p, const double* h, double* out, int64_t cap, int64_t* n);
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A);
 BSGPU_API int bsgpu_matrix_get_info(bsgpu_matrix_t A, int64_t* nrows, int64_t* nb, int64_t* nnzb, int32_t* Np);
 /* Copies the values back in the creation layout (row-major blocks) to a host or device buffer. */
