@@ -10,7 +10,7 @@ from helpers import random_var_bsr
 
 pytestmark = pytest.mark.gpu
 
-SOL_TOL = 1e-9  # relative L2 error of solutions against the FP64 direct solve (north-star criterion)
+SOL_TOL = 1e-9  # relative L2 error of solutions against the FP64 direct solve (the solution criterion)
 
 
 def test_change_of_basis_matches_oracle(cuda):

@@ -9,7 +9,7 @@ from helpers import random_var_bsr
 
 pytestmark = pytest.mark.gpu
 
-TOL = 1e-13  # relative, FP64 (north-star SpMV criterion)
+TOL = 1e-13  # relative, FP64 (the SpMV parity criterion)
 
 
 def _check(system, alpha, beta, seed=0):
