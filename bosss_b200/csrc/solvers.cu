@@ -80,11 +80,10 @@ long long Ctx::capture_leave() {
 }
 
 void Ctx::capture_begin() {
-  graph_init();
+  graph_init();  // allocations before the capture (capture_join finds them made)
   BSGPU_CUDA(cudaStreamSynchronize(st));
-  capture_join();
   BSGPU_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-  mark = launches_now();
+  capture_join();
 }
 
 long long Ctx::capture_end(cudaGraph_t* g) {
