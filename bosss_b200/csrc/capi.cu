@@ -288,6 +288,34 @@ BSGPU_API int bsgpu_sip_templates(int32_t D, int32_t p, const double* h, double*
   });
 }
 
+BSGPU_API int bsgpu_schwarz_blocks(int64_t nb, const int64_t* row_ptr, const int32_t* col_idx, int64_t parts,
+                                   int32_t overlap, int64_t* ptr, int32_t* cells, int64_t* nblocks, int64_t* total) {
+  return guarded([&] {
+    require(nb >= 0 && row_ptr != nullptr && (col_idx != nullptr || nb == 0), "null argument");
+    Matrix M;  // host structure only: no device memory is touched
+    M.nb = nb;
+    M.h_rp.assign(row_ptr, row_ptr + nb + 1);
+    M.nnzb = M.h_rp[nb];
+    M.h_ci.assign(col_idx, col_idx + M.nnzb);
+    for (int64_t k = 0; k < M.nnzb; ++k)
+      require(M.h_ci[k] >= 0 && M.h_ci[k] < nb, "column index out of range");
+    auto blocks = schwarz_partition(M, parts > 0 ? parts : std::max<int64_t>(1, (nb + 7) / 8));
+    schwarz_extend(M, blocks, overlap);
+    int64_t n = 0;
+    for (auto& bl : blocks) n += (int64_t)bl.size();
+    if (nblocks) *nblocks = (int64_t)blocks.size();
+    if (total) *total = n;
+    if (ptr && cells) {
+      int64_t o = 0;
+      ptr[0] = 0;
+      for (size_t b = 0; b < blocks.size(); ++b) {
+        for (int32_t c : blocks[b]) cells[o++] = c;
+        ptr[b + 1] = o;
+      }
+    }
+  });
+}
+
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A) {
   return guarded([&] {
     if (A && !A->borrowed) delete A;

@@ -89,6 +89,12 @@ BSGPU_API int bsgpu_assemble_sip_cartesian(bsgpu_matrix_t* A, int32_t D, const i
  * direction d; 13+6d .. 15+6d: the off-diagonal terms of direction d).  n (may be NULL): entries; out (may be NULL
  * to query n) holds cap entries. */
 BSGPU_API int bsgpu_sip_templates(int32_t D, int32_t p, const double* h, double* out, int64_t cap, int64_t* n);
+/* The cell blocks of BSGPU_SMOOTHER_SCHWARZ_BLOCKS for a block structure (host computation, no device work): the
+ * partition into `parts` blocks (0: blocks of 8 cells; greedy breadth-first aggregation of the block graph, the
+ * stand-in for METISBlockingStrategy, Schwarz.cs:190-320) grown by `overlap` layers (Schwarz.cs:690-735), each
+ * block's cells ascending.  ptr[nblocks + 1] and cells[total] (both NULL: sizes only). */
+BSGPU_API int bsgpu_schwarz_blocks(int64_t nb, const int64_t* row_ptr, const int32_t* col_idx, int64_t parts,
+                                   int32_t overlap, int64_t* ptr, int32_t* cells, int64_t* nblocks, int64_t* total);
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A);
 BSGPU_API int bsgpu_matrix_get_info(bsgpu_matrix_t A, int64_t* nrows, int64_t* nb, int64_t* nnzb, int32_t* Np);
 /* Copies the values back in the creation layout (row-major blocks) to a host or device buffer. */

@@ -1278,6 +1278,32 @@ int or_ilu0_solve(const or_bsr* m, const int32_t* order, const double* factor, c
   }
 }
 
+int or_schwarz_blocks(const or_bsr* m, int64_t parts, int overlap, int64_t* ptr, int32_t* cells, int64_t* nblocks,
+                      int64_t* total) {
+  try {
+    Mat A;
+    load_mat(A, m);
+    auto blocks = schwarz_partition_mat(A, parts > 0 ? parts : std::max<int64_t>(1, (A.nb + 7) / 8));
+    schwarz_extend_mat(A, blocks, overlap);
+    int64_t n = 0;
+    for (auto& bl : blocks) n += (int64_t)bl.size();
+    if (nblocks) *nblocks = (int64_t)blocks.size();
+    if (total) *total = n;
+    if (ptr && cells) {
+      int64_t o = 0;
+      ptr[0] = 0;
+      for (size_t b = 0; b < blocks.size(); ++b) {
+        for (int32_t c : blocks[b]) cells[o++] = c;
+        ptr[b + 1] = o;
+      }
+    }
+    return 0;
+  } catch (std::exception& e) {
+    g_err = e.what();
+    return OR_ERR_ARITHMETIC;
+  }
+}
+
 int or_block_schwarz(const or_bsr* m, int64_t parts, int overlap, int scaling, int iters, double* x, const double* b) {
   try {
     Mat A;

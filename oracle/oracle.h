@@ -57,6 +57,10 @@ int or_blockjacobi(const or_bsr* m, int iters, double omega, double* x, const do
 /* additive Schwarz with multi-cell blocks: `parts` greedy breadth-first blocks (0: 8 cells each) grown by
  * `overlap` layers, dense block solves, optional overlap scaling; `iters` updates of x */
 int or_block_schwarz(const or_bsr* m, int64_t parts, int overlap, int scaling, int iters, double* x, const double* b);
+/* the cell lists of the multi-cell Schwarz blocks (partition into `parts` blocks, 0: blocks of 8 cells; grown by
+   `overlap` layers): ptr[nblocks + 1], cells[total]; null ptr/cells: sizes only */
+int or_schwarz_blocks(const or_bsr* m, int64_t parts, int overlap, int64_t* ptr, int32_t* cells, int64_t* nblocks,
+                      int64_t* total);
 int or_schwarz_rows(const or_bsr* m, double* values_out);
 /* block ILU(0) over the block rows in `order` (NULL: natural order); factors in the matrix layout */
 int or_ilu0_factor(const or_bsr* m, const int32_t* order, double* factor_out);

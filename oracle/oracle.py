@@ -182,6 +182,19 @@ def ilu0_solve(A: Bsr, factor: np.ndarray, b: np.ndarray, order=None) -> np.ndar
     return x
 
 
+def schwarz_blocks(A: Bsr, parts: int = 0, overlap: int = 1):
+    """Cell lists of the multi-cell Schwarz blocks (or_schwarz_blocks): (ptr [nblocks+1], cells)."""
+    lib().or_schwarz_blocks.argtypes = [C.c_void_p, C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]
+    nb, tot = C.c_int64(), C.c_int64()
+    _check(lib().or_schwarz_blocks(C.byref(A._c), int(parts), int(overlap), None, None, C.byref(nb), C.byref(tot)))
+    ptr = np.zeros(nb.value + 1, np.int64)
+    cells = np.zeros(max(tot.value, 1), np.int32)
+    _check(lib().or_schwarz_blocks(C.byref(A._c), int(parts), int(overlap), ptr.ctypes.data, cells.ctypes.data,
+                                   None, None))
+    return ptr, cells[:tot.value]
+
+
 def block_schwarz(A: Bsr, x: np.ndarray, b: np.ndarray, parts: int = 0, overlap: int = 1, scaling: bool = False,
                   iters: int = 1) -> np.ndarray:
     """Additive Schwarz with multi-cell blocks (Schwarz.cs:56): `iters` updates of x."""
