@@ -316,6 +316,26 @@ BSGPU_API int bsgpu_schwarz_blocks(int64_t nb, const int64_t* row_ptr, const int
   });
 }
 
+BSGPU_API int bsgpu_ilu_wavefronts(int64_t nb, const int64_t* row_ptr, const int32_t* col_idx, int64_t* level_ptr,
+                                   int32_t* rows, int64_t* nlevels) {
+  return guarded([&] {
+    require(nb >= 0 && row_ptr != nullptr && (col_idx != nullptr || nb == 0), "null argument");
+    Matrix M;  // host structure only: no device memory is touched
+    M.nb = nb;
+    M.h_rp.assign(row_ptr, row_ptr + nb + 1);
+    M.nnzb = M.h_rp[nb];
+    M.h_ci.assign(col_idx, col_idx + M.nnzb);
+    for (int64_t k = 0; k < M.nnzb; ++k)
+      require(M.h_ci[k] >= 0 && M.h_ci[k] < nb, "column index out of range");
+    std::vector<int64_t> lptr;
+    std::vector<int32_t> order;
+    ilu_wavefronts(M, lptr, order);
+    if (nlevels) *nlevels = (int64_t)lptr.size() - 1;
+    if (level_ptr) std::copy(lptr.begin(), lptr.end(), level_ptr);
+    if (rows) std::copy(order.begin(), order.end(), rows);
+  });
+}
+
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A) {
   return guarded([&] {
     if (A && !A->borrowed) delete A;

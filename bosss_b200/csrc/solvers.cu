@@ -9,6 +9,28 @@
 
 namespace bsgpu {
 
+// Wavefronts of the natural-order block ILU(0) (CellILU.cs:1229-1330): a block row's wavefront is one more than the
+// largest wavefront of its lower neighbours, so the rows of one wavefront depend only on earlier ones.  lptr: offsets
+// of the wavefronts in `order` (rows ascending within a wavefront).
+void ilu_wavefronts(const Matrix& A, std::vector<int64_t>& lptr, std::vector<int32_t>& order) {
+  const int64_t nb = A.nb;
+  std::vector<int32_t> lev(nb, 0);
+  int nlev = nb ? 1 : 0;
+  for (int64_t i = 0; i < nb; ++i) {
+    for (int64_t k = A.h_rp[i]; k < A.h_rp[i + 1]; ++k) {
+      const int32_t j = A.h_ci[k];
+      if (j < i) lev[i] = std::max(lev[i], lev[j] + 1);
+    }
+    nlev = std::max(nlev, lev[i] + 1);
+  }
+  lptr.assign(nlev + 1, 0);
+  for (int64_t i = 0; i < nb; ++i) lptr[lev[i] + 1]++;
+  for (int l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];
+  order.assign(nb, 0);
+  std::vector<int64_t> fillp(lptr.begin(), lptr.end() - 1);
+  for (int64_t i = 0; i < nb; ++i) order[fillp[lev[i]]++] = (int32_t)i;
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------------------------------------------
@@ -448,21 +470,8 @@ struct ILUNaturalT : Solver<T> {
     require(A64->uniform && (A64->Np == 4 || A64->Np == 6 || A64->Np == 10 || A64->Np == 20),
             "natural-order ILU needs uniform blocks of 4, 6, 10 or 20", BSGPU_ERR_UNSUPPORTED);
     const int64_t nb = A64->nb;
-    std::vector<int32_t> lev(nb, 0);
-    int nlev = nb ? 1 : 0;
-    for (int64_t i = 0; i < nb; ++i) {
-      for (int64_t k = A64->h_rp[i]; k < A64->h_rp[i + 1]; ++k) {
-        const int32_t j = A64->h_ci[k];
-        if (j < i) lev[i] = std::max(lev[i], lev[j] + 1);
-      }
-      nlev = std::max(nlev, lev[i] + 1);
-    }
-    lptr.assign(nlev + 1, 0);
-    for (int64_t i = 0; i < nb; ++i) lptr[lev[i] + 1]++;
-    for (int l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];
-    std::vector<int32_t> order(nb);
-    std::vector<int64_t> fillp(lptr.begin(), lptr.end() - 1);
-    for (int64_t i = 0; i < nb; ++i) order[fillp[lev[i]]++] = (int32_t)i;
+    std::vector<int32_t> order;
+    ilu_wavefronts(*A64, lptr, order);
     rows.alloc(std::max<int64_t>(nb, 1));
     if (nb) BSGPU_CUDA(cudaMemcpy(rows.p, order.data(), nb * 4, cudaMemcpyHostToDevice));
     const std::vector<int64_t> o = diag_offsets(*A64);

@@ -167,6 +167,8 @@ struct Tree {
   int learned_pool = 0;             // training residuals collected by the last train_learned
 };
 Tree* build_tree(const Matrix* A, const bsgpu_solver_config& cfg, const OperatorInfo& info);
+// wavefronts of the natural-order block ILU(0) from the host block structure (lptr offsets into order)
+void ilu_wavefronts(const Matrix& A, std::vector<int64_t>& lptr, std::vector<int32_t>& order);
 
 // The whole FlexGMRES solve recorded into a CUDA graph (cfg.graph == 2): restart and Arnoldi loops as WHILE nodes,
 // the preconditioners' round-robin as IF nodes, every decision on the device (devctl.cuh FgState), the V-cycle

@@ -95,6 +95,12 @@ BSGPU_API int bsgpu_sip_templates(int32_t D, int32_t p, const double* h, double*
  * block's cells ascending.  ptr[nblocks + 1] and cells[total] (both NULL: sizes only). */
 BSGPU_API int bsgpu_schwarz_blocks(int64_t nb, const int64_t* row_ptr, const int32_t* col_idx, int64_t parts,
                                    int32_t overlap, int64_t* ptr, int32_t* cells, int64_t* nblocks, int64_t* total);
+/* The wavefronts of BSGPU_SMOOTHER_ILU_NATURAL for a block structure (host computation, no device work): a block
+ * row's wavefront is one more than the largest of its lower neighbours' (the dependency levels of CellILU's natural
+ * order, CellILU.cs:1229-1330).  level_ptr[nlevels + 1] offsets into rows[nb] (ascending within a wavefront); pass
+ * NULL outputs to query nlevels. */
+BSGPU_API int bsgpu_ilu_wavefronts(int64_t nb, const int64_t* row_ptr, const int32_t* col_idx, int64_t* level_ptr,
+                                   int32_t* rows, int64_t* nlevels);
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A);
 BSGPU_API int bsgpu_matrix_get_info(bsgpu_matrix_t A, int64_t* nrows, int64_t* nb, int64_t* nnzb, int32_t* Np);
 /* Copies the values back in the creation layout (row-major blocks) to a host or device buffer. */
