@@ -620,6 +620,44 @@ class SineModes:
              for d in range(3)]                                                     # [cells, M, n1]
         return np.einsum("m,kmi,kmj,kml->kijl", self.a, S[0], S[1], S[2], optimize=True)
 
+    def tables_1d(self, grid: RectilinearGrid, p: int, q: Optional[int] = None) -> np.ndarray:
+        """The 1-D projections of every mode and direction, [M, D, n_d, p+1] (grids with equal extents; the
+        per-cell load vector is the product over the directions summed over the modes, as in ``project``)."""
+        D = grid.D
+        q = q if q is not None else p + 6
+        tg, wg = gauss(q)
+        vals = np.stack([psi(j, tg) for j in range(p + 1)], axis=-1)  # [q, p+1]
+        out = []
+        for m in range(len(self.a)):
+            per_d = []
+            for d in range(D):
+                n = np.asarray(grid.nodes[d], dtype=np.float64)
+                h = np.diff(n)
+                xq = 0.5 * (n[:-1] + n[1:])[:, None] + 0.5 * h[:, None] * tg[None, :]
+                I = (np.sin(math.pi * self.k[m, d] * xq) * wg[None, :]) @ vals
+                per_d.append(I * (0.5 * h * np.sqrt(2.0 / h))[:, None])
+            out.append(per_d)
+        return out
+
+    def project_on_gpu(self, grid: RectilinearGrid, p: int, q: Optional[int] = None, out=None):
+        """``project`` with the products and mode sums evaluated on the GPU (bsgpu_project_separable); returns a
+        CUDA tensor [cells * Np] (or fills ``out``)."""
+        import ctypes as C
+        import torch
+        from . import native as nat
+        D = grid.D
+        tabs = self.tables_1d(grid, p, q)
+        flat = np.concatenate([np.ascontiguousarray(tabs[m][d]).reshape(-1)
+                               for m in range(len(self.a)) for d in range(D)]) if len(self.a) else np.zeros(1)
+        coef = np.ascontiguousarray(self.a, np.float64)
+        Np = np_of(D, p)
+        if out is None:
+            out = torch.empty(grid.ncells * Np, dtype=torch.float64, device="cuda")
+        shape = (C.c_int32 * D)(*grid.shape)
+        nat.check(nat.lib().bsgpu_project_separable(D, shape, int(p), len(self.a), nat.ptr(coef), nat.ptr(flat),
+                                                    nat.ptr(out), nat.DEVICE_POINTERS))
+        return out
+
     def project(self, grid: RectilinearGrid, p: int, q: Optional[int] = None) -> np.ndarray:
         """Separable projection: per mode and direction a 1-D Gauss integral, combined by outer products."""
         D = grid.D

@@ -13,6 +13,7 @@
 // The host computes the templates (Gauss-Legendre quadrature of the 1-D stiffness matrix, traces at +-1); one thread
 // per block entry keeps its entries of all templates in registers and writes that entry of every block of a range of
 // cells (coalesced: the threads of a CTA write whole blocks).
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdint>
@@ -256,6 +257,11 @@ std::vector<double> sip_templates(int D, int p, const double* h) {
 
 int sip_template_count() { return kTemplates; }
 
+int modes_count(int D, int p) {
+  require(D >= 1 && D <= 3 && p >= 0, "D must be 1, 2 or 3 and p >= 0");
+  return (int)modes_of(D, p).size();
+}
+
 Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi, int p, double penalty,
                                const double* nu, bool nu_device) {
   require(D >= 1 && D <= 3, "D must be 1, 2 or 3");
@@ -328,6 +334,76 @@ Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi
   BSGPU_CHECK_LAUNCH();
   BSGPU_CUDA(cudaDeviceSynchronize());
   return matrix_create(nc, Np, nullptr, d_rp.p, d_ci.p, d_vals.p, BSGPU_DEVICE_POINTERS);
+}
+
+}  // namespace bsgpu
+
+namespace bsgpu {
+
+namespace {
+
+// out[c * Np + a] = sum_m coef[m] prod_d T[((m * D + d) * nmax + i_d(c)) * (p + 1) + mode_a[d]]
+__global__ void separable_projection_kernel(int D, int n0, int n1, int n2, int p, int Np, int M, int nmax,
+                                            const int* __restrict__ modes, const double* __restrict__ coef,
+                                            const double* __restrict__ T, int64_t nc, double* __restrict__ out) {
+  const int64_t total = nc * Np;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < total; g += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = g / Np;
+    const int a = (int)(g - c * Np);
+    const int i0 = (int)(c % n0);
+    const int i1 = (int)((c / n0) % n1);
+    const int i2 = (int)(c / ((int64_t)n0 * n1));
+    const int idx[3] = {i0, i1, i2};
+    double s = 0.0;
+    for (int m = 0; m < M; ++m) {
+      double t = coef[m];
+      for (int d = 0; d < D; ++d)
+        t *= T[((int64_t)(m * D + d) * nmax + idx[d]) * (p + 1) + modes[a * 3 + d]];
+      s += t;
+    }
+    out[g] = s;
+  }
+  (void)n2;
+}
+
+}  // namespace
+
+void project_separable(int D, const int32_t* shape, int p, int M, const double* coef, const double* tables,
+                       double* out_device, cudaStream_t st) {
+  require(D >= 1 && D <= 3, "D must be 1, 2 or 3");
+  require(p >= 0 && M >= 0, "p and the term count must be >= 0");
+  int n[3] = {1, 1, 1};
+  int64_t nc = 1;
+  int nmax = 1;
+  for (int d = 0; d < D; ++d) {
+    require(shape[d] >= 1, "every grid extent must be >= 1");
+    n[d] = shape[d];
+    nc *= shape[d];
+    nmax = std::max(nmax, shape[d]);
+  }
+  const auto modes = modes_of(D, p);
+  const int Np = (int)modes.size();
+  std::vector<int> mflat((size_t)Np * 3);
+  for (int a = 0; a < Np; ++a)
+    for (int d = 0; d < 3; ++d) mflat[(size_t)a * 3 + d] = modes[a][d];
+  // the caller's tables are [M][D][n_d][p + 1]; repack to a common stride nmax per direction
+  std::vector<double> T((size_t)std::max(M, 1) * D * nmax * (p + 1), 0.0);
+  size_t src = 0;
+  for (int m = 0; m < M; ++m)
+    for (int d = 0; d < D; ++d)
+      for (int i = 0; i < n[d]; ++i)
+        for (int j = 0; j <= p; ++j) T[(((size_t)m * D + d) * nmax + i) * (p + 1) + j] = tables[src++];
+  DBuf<int> d_modes(mflat.size());
+  DBuf<double> d_coef(std::max(M, 1)), d_T(T.size());
+  BSGPU_CUDA(cudaMemcpy(d_modes.p, mflat.data(), mflat.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (M) BSGPU_CUDA(cudaMemcpy(d_coef.p, coef, M * 8, cudaMemcpyHostToDevice));
+  BSGPU_CUDA(cudaMemcpy(d_T.p, T.data(), T.size() * 8, cudaMemcpyHostToDevice));
+  const int64_t total = nc * Np;
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)num_sms() * 16));
+  separable_projection_kernel<<<grid, 256, 0, st>>>(D, n[0], n[1], n[2], p, Np, M, nmax, d_modes.p, d_coef.p,
+                                                   d_T.p, nc, out_device);
+  BSGPU_CHECK_LAUNCH();
+  BSGPU_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace bsgpu

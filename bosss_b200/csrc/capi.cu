@@ -336,6 +336,24 @@ BSGPU_API int bsgpu_ilu_wavefronts(int64_t nb, const int64_t* row_ptr, const int
   });
 }
 
+BSGPU_API int bsgpu_project_separable(int32_t D, const int32_t* shape, int32_t p, int32_t M, const double* coef,
+                                      const double* tables, double* out, int32_t flags) {
+  return guarded([&] {
+    require(shape && out && (M == 0 || (coef && tables)), "null argument");
+    require(flags == BSGPU_HOST_POINTERS || flags == BSGPU_DEVICE_POINTERS, "bad pointer flag");
+    int64_t nc = 1;
+    for (int d = 0; d < D && d < 3; ++d) nc *= std::max(shape[d], 1);
+    const int64_t N = nc * (int64_t)modes_count(D, p);
+    if (flags == BSGPU_DEVICE_POINTERS) {
+      project_separable(D, shape, p, M, coef, tables, out, nullptr);
+    } else {
+      DBuf<double> d(std::max<int64_t>(N, 1));
+      project_separable(D, shape, p, M, coef, tables, d.p, nullptr);
+      BSGPU_CUDA(cudaMemcpy(out, d.p, N * 8, cudaMemcpyDeviceToHost));
+    }
+  });
+}
+
 BSGPU_API int bsgpu_matrix_destroy(bsgpu_matrix_t A) {
   return guarded([&] {
     if (A && !A->borrowed) delete A;

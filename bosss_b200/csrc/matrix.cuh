@@ -71,6 +71,12 @@ Matrix* assemble_sip_cartesian(int D, const int32_t* shape, double lo, double hi
 // 13 + 6d .. 15 + 6d the off-diagonal terms of direction d)
 std::vector<double> sip_templates(int D, int p, const double* h);
 int sip_template_count();
+int modes_count(int D, int p);  // modes of total degree <= p in D dimensions
+// load vector of a separable right-hand side sum_m coef[m] prod_d f_{m,d}(x_d) on a Cartesian grid: tables holds the
+// 1-D projections [M][D][shape[d]][p + 1] (integral of f_{m,d} times the 1-D basis over each cell interval, with
+// the 1-D scaling); out_device[c * Np + a] = sum_m coef[m] prod_d tables[m][d][i_d(c)][mode_a[d]]
+void project_separable(int D, const int32_t* shape, int p, int M, const double* coef, const double* tables,
+                       double* out_device, cudaStream_t st);
 
 // y = alpha*A*x + beta*z (z may be y; z == nullptr: beta ignored).  `active`: optional device flag, the launch
 // is a no-op when *active == 0.

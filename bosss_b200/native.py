@@ -38,7 +38,7 @@ EXPORTS = [
     "bsgpu_solver_learned_info", "bsgpu_solver_learned_get_weights", "bsgpu_solver_learned_set_weights",
     "bsgpu_solver_learned_apply", "bsgpu_solver_learned_gradient",
     "bsgpu_batch_create", "bsgpu_batch_solve_device", "bsgpu_batch_destroy", "bsgpu_assemble_sip_cartesian",
-    "bsgpu_sip_templates", "bsgpu_schwarz_blocks", "bsgpu_ilu_wavefronts",
+    "bsgpu_sip_templates", "bsgpu_schwarz_blocks", "bsgpu_ilu_wavefronts", "bsgpu_project_separable",
 ]
 
 
@@ -131,6 +131,7 @@ def lib() -> C.CDLL:
             "bsgpu_sip_templates": [i32, i32, vp, vp, i64, vp],
             "bsgpu_schwarz_blocks": [i64, vp, vp, i64, i32, vp, vp, vp, vp],
             "bsgpu_ilu_wavefronts": [i64, vp, vp, vp, vp, vp],
+            "bsgpu_project_separable": [i32, vp, i32, i32, vp, vp, vp, i32],
         }
         for name, args in sig.items():
             f = getattr(L, name)

@@ -84,6 +84,13 @@ BSGPU_API int bsgpu_matrix_create(bsgpu_matrix_t* A, int64_t nb, int32_t Np, con
  * diffusivity (NULL: 1), a host or device array per flags (BSGPU_HOST_POINTERS / BSGPU_DEVICE_POINTERS). */
 BSGPU_API int bsgpu_assemble_sip_cartesian(bsgpu_matrix_t* A, int32_t D, const int32_t* shape, double lo, double hi,
                                            int32_t p, double penalty, const double* nu, int32_t flags);
+/* Load vector of a separable right-hand side f(x) = sum_m coef[m] prod_d f_{m,d}(x_d) on the same grid and basis:
+ * tables holds, per term m and direction d, the 1-D projections of f_{m,d} onto the 1-D basis of every cell
+ * interval, [M][D][shape[d]][p + 1] (the integral over the interval of f_{m,d} times the scaled 1-D Legendre
+ * function); out[c * Np + a] = sum_m coef[m] prod_d tables[m][d][i_d(c)][mode_a[d]], a host or device array per
+ * flags.  (The benchmark's sine-mode right-hand sides are of this form.) */
+BSGPU_API int bsgpu_project_separable(int32_t D, const int32_t* shape, int32_t p, int32_t M, const double* coef,
+                                      const double* tables, double* out, int32_t flags);
 /* The block templates of that assembly for cell sizes h[0..D) (host computation, no device work): 31 row-major
  * Np x Np matrices (0: volume term; 1+4d .. 4+4d: consistency and penalty terms of the +d and -d faces of
  * direction d; 13+6d .. 15+6d: the off-diagonal terms of direction d).  n (may be NULL): entries; out (may be NULL

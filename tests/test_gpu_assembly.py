@@ -70,3 +70,15 @@ def test_solve_on_gpu_assembled_operator(cuda):
     xd = O.direct_solve(s)
     assert slv.Converged
     assert np.linalg.norm(x - xd) <= 1e-9 * np.linalg.norm(xd)
+
+
+@pytest.mark.parametrize("shape,p", [((9,), 3), ((6, 5), 3), ((5, 4, 3), 2), ((4, 4, 4), 3)])
+def test_load_vector_on_gpu_matches_host(cuda, shape, p):
+    """The sine-mode load vector with its products and mode sums on the GPU (bsgpu_project_separable) against the
+    host projection (SineModes.project) to 1e-14 relative."""
+    g = _grid(shape)
+    sm = A.SineModes.seeded(5, len(shape))
+    ref = sm.project(g, p).reshape(-1)
+    got = sm.project_on_gpu(g, p).cpu().numpy()
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() <= 1e-14 * np.abs(ref).max()
