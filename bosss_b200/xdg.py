@@ -22,7 +22,7 @@ import math
 
 import numpy as np
 
-from .assembly import (RectilinearGrid, SineModes, _expand_1d, _face_vectors, dg_modes, dpsi, gauss, psi,
+from .assembly import (RectilinearGrid, SineModes, _expand_1d, dg_modes, dpsi, gauss, psi,
                        stiffness_1d, uniform_grid)
 
 
