@@ -329,3 +329,40 @@ def test_block_schwarz_single_block_is_exact_and_overlap_sums():
     bj = O.block_schwarz(Bo, np.zeros(s.N), s.rhs, parts=s.nb, overlap=0, iters=1)
     ref = O.blockjacobi(Bo, np.zeros(s.N), s.rhs, iters=0)
     assert np.linalg.norm(bj - ref) <= 1e-12 * np.linalg.norm(ref)
+
+
+def test_fgmres_restart_cycles_and_iteration_limit():
+    """FlexGMRES with a Krylov dimension of 3 (restart cycles every 3 steps) still reaches the direct solution; with
+    MaxSolverIterations = 4 it stops unconverged after at most 4 preconditioner applications (the limit test of
+    IterativeSolverConfig.cs:55)."""
+    s = A.poisson_3d(4, 2)
+    Bt, Lcat, bl = _transformed(s)
+    bt = apply_blocks(Lcat, bl, s.rhs)
+    base = dict(solver=O.FGMRES_PMG, top_mode=O.TERM_RELATIVE, level_keep=(10, 4, 1), coarse_kind=O.COARSE_PCG,
+                coarse_tol=0.5, coarse_max_iter=2, post_sweeps=1, sub_max_iter=1)
+    r = O.solve(Bt, bt, O.SolverConfig(tol=1e-11, max_krylov=3, **base))
+    x = apply_blocks(Lcat, bl, r.x, transpose=True)
+    xd = O.direct_solve(s)
+    assert r.converged and r.iterations > 3
+    assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
+    lim = O.solve(Bt, bt, O.SolverConfig(tol=1e-14, max_krylov=3, max_iter=4, **base))
+    assert not lim.converged and lim.iterations <= 5
+
+
+def test_default_termination_absolute_floor():
+    """DefaultTermination (IterativeSolverConfig.cs:48-62): R < R0 tol + tol.  For a right-hand side of norm 1e-9
+    the absolute part (1e-10) ends the solve after a reduction of about 10, the relative form continues to its own
+    tolerance or the machine-precision floor 2.2e-13."""
+    s = A.poisson_3d(4, 1)
+    Bt, Lcat, bl = _transformed(s)
+    bt = apply_blocks(Lcat, bl, s.rhs)
+    bt = bt / np.linalg.norm(bt) * 1e-9
+    # a weak preconditioner (one sweep, two coarse CG steps), so that the residual falls gradually
+    cfg = dict(solver=O.FGMRES_PMG, tol=1e-10, level_keep=(4, 1), coarse_kind=O.COARSE_PCG, coarse_tol=0.5,
+               coarse_max_iter=2, post_sweeps=1, sub_max_iter=1)
+    absolute = O.solve(Bt, bt, O.SolverConfig(top_mode=O.TERM_DEFAULT, **cfg))
+    relative = O.solve(Bt, bt, O.SolverConfig(top_mode=O.TERM_RELATIVE, **cfg))
+    assert absolute.converged and relative.converged
+    assert absolute.res < absolute.res0 * 1e-10 + 1e-10
+    assert relative.res < max(relative.res0 * 1e-10, 2.2205e-13)
+    assert relative.iterations > absolute.iterations
